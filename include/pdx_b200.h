@@ -1,0 +1,131 @@
+/*
+ * pdx_b200.h -- C ABI of the B200 PDX search engine (libpdx_b200.so).
+ *
+ * Drop-in boundary for the reference's search path: every entry point below replaces one
+ * member of the reference's C++ index interface (include/pdx/index.hpp) or of its pybind
+ * surface (include/pdx/lib/lib.hpp, python/lib.cpp), with plain pointers and sizes instead of
+ * C++ / numpy types. Status codes are returned, never thrown; pdxg_last_error() describes the
+ * last failure on the calling thread.
+ *
+ * Index files are the reference's own serialized format (PDXIndex/PDXTreeIndex::Save,
+ * index.hpp:213-239 and 483-514); an index is loaded once into GPU memory and searched there.
+ * The search path has no CPU fallback: without a usable CUDA device every call fails with
+ * PDXG_ERR_CUDA.
+ */
+#ifndef PDX_B200_H
+#define PDX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pdxg_index pdxg_index;
+
+/* Status codes. */
+#define PDXG_OK 0
+#define PDXG_ERR_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define PDXG_ERR_IO 2               /* file missing / unreadable / truncated */
+#define PDXG_ERR_FORMAT 3           /* unknown index type or inconsistent header */
+#define PDXG_ERR_CUDA 4             /* CUDA runtime failure (no device, launch error, OOM) */
+#define PDXG_ERR_UNSUPPORTED 5      /* operation not available for this index type */
+#define PDXG_ERR_CAPACITY 6         /* request exceeds a stated engine limit */
+
+/* Index types: the type byte of the file (common.hpp:78, PDXIndexType). */
+#define PDXG_TYPE_F32 0
+#define PDXG_TYPE_U8 1
+#define PDXG_TYPE_TREE_F32 2
+#define PDXG_TYPE_TREE_U8 3
+
+/* Search flags. */
+#define PDXG_QUERY_TRANSFORMED 1u /* queries are already normalized + rotated: the reference's
+                                     Search(query, k, is_query_transformed = true),
+                                     searcher.hpp:596-613 */
+
+/* Last error message of the calling thread (never NULL). */
+const char* pdxg_last_error(void);
+
+/* Replaces LoadPDXIndex(path) (index.hpp:1736-1760) + Restore (index.hpp:242-267, 516-543) and
+ * the pybind module function load_index (python/lib.cpp:52-57). Loads the file into GPU memory
+ * on `device`. */
+int pdxg_load(const char* path, int device, pdxg_index** out);
+
+/* Same as pdxg_load, from an in-memory copy of the file bytes. */
+int pdxg_load_buffer(const void* data, uint64_t size, int device, pdxg_index** out);
+
+/* Releases the index and its GPU memory. NULL is ignored. */
+void pdxg_free(pdxg_index* index);
+
+/* Replaces IPDXIndex::SetNProbe (index.hpp:171, 282) / PDXIndex.set_nprobe (lib.cpp:41).
+ * 0 means "all clusters", as in PDXearch::Search (searcher.hpp:614-616). */
+int pdxg_set_nprobe(pdxg_index* index, uint32_t nprobe);
+
+/* Replaces ADSamplingPruner::SetPruningAggresiveness (adsampling.hpp:80-85): epsilon0 of the
+ * ADSampling bound (default 1.5, common.hpp:67). Very large values disable pruning. */
+int pdxg_set_pruning_aggressiveness(pdxg_index* index, float epsilon0);
+
+/* Replaces IPDXIndex::Search (index.hpp:167, 269-271, 545-566) and PDXIndex.search
+ * (lib.hpp:92-112), batched: `queries` is nq x d row-major float32 in HOST memory; results go
+ * to host arrays ids[nq*k], distances[nq*k] (ascending per query; unused slots hold
+ * UINT32_MAX / +inf) and counts[nq]. Synchronous. */
+int pdxg_search(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
+                uint32_t* ids, float* distances, uint32_t* counts);
+
+/* Device-resident variant of pdxg_search: every pointer is GPU memory on the index's device;
+ * the work is enqueued on `stream` (a cudaStream_t, NULL = the index's own stream) and the call
+ * returns without waiting. Workspace is allocated on first use and reused. */
+int pdxg_search_device(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k,
+                       uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts,
+                       void* stream);
+
+/* Replaces PDXearch::SetClusterAccessOrder (searcher.hpp:48-54) followed by Search: visits the
+ * given clusters (at most nprobe of them) in the given order instead of probing centroids.
+ * Host pointers, synchronous. */
+int pdxg_search_with_order(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k,
+                           const uint32_t* order, uint32_t n_order, uint32_t flags, uint32_t* ids,
+                           float* distances, uint32_t* counts);
+
+/* Replaces IPDXIndex::FilteredSearch (index.hpp:168-172, 273-280, 568-578) and
+ * PDXIndex.filtered_search (lib.hpp:114-142): one query, only rows whose id is listed in
+ * row_ids[n_row_ids] can be returned. Host pointers, synchronous; *count receives the number
+ * of results written to ids[k] / distances[k]. Unknown row ids are ignored. */
+int pdxg_filtered_search(pdxg_index* index, const float* query, uint32_t k,
+                         const uint64_t* row_ids, uint64_t n_row_ids, uint32_t flags,
+                         uint32_t* ids, float* distances, uint32_t* count);
+
+/* Batched filtered search: nq queries, each with its own row-id list. Query q uses
+ * row_ids[offsets[q] .. offsets[q+1]) (offsets has nq+1 entries); offsets[q] == UINT64_MAX
+ * marks query q as unfiltered. Host pointers, synchronous. */
+int pdxg_filtered_search_batch(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k,
+                               const uint64_t* row_ids, const uint64_t* offsets, uint32_t flags,
+                               uint32_t* ids, float* distances, uint32_t* counts);
+
+/* Replaces IPDXIndex::Save (index.hpp:173, 213-239, 483-514): writes the reference's format. */
+int pdxg_save(pdxg_index* index, const char* path);
+
+/* Getters: IPDXIndex::GetNumDimensions / GetNumClusters / GetClusterSize / GetClusterRowIds /
+ * GetInMemorySizeInBytes (index.hpp:175-179) and the pybind getters (lib.hpp:148-164). */
+int pdxg_index_type(const pdxg_index* index);
+uint32_t pdxg_num_dimensions(const pdxg_index* index);
+uint32_t pdxg_num_clusters(const pdxg_index* index);
+uint32_t pdxg_nprobe(const pdxg_index* index);
+uint32_t pdxg_cluster_size(const pdxg_index* index, uint32_t cluster_id);
+int pdxg_cluster_row_ids(const pdxg_index* index, uint32_t cluster_id, uint32_t* out,
+                         uint32_t capacity);
+uint64_t pdxg_in_memory_size_in_bytes(const pdxg_index* index);
+uint64_t pdxg_num_embeddings(const pdxg_index* index);
+
+/* Rotated (normalized when the index is) queries, as the search sees them: the reference's
+ * ADSamplingPruner::PreprocessQuery (adsampling.hpp:100-113) on nq host queries. */
+int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, float* out);
+
+/* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
+int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDX_B200_H */

@@ -1,0 +1,329 @@
+"""ctypes binding of libpdx_b200.so with the reference's pybind surface.
+
+Mirrors module `pdxearch.compiled` (python/lib.cpp:6-60, include/pdx/lib/lib.hpp:15-175):
+class `PDXIndex` with the same constructor arguments and methods, and `load_index(path)`.
+Errors map like pybind's: invalid arguments -> ValueError, everything else -> RuntimeError.
+
+There is no CPU fallback: if the CUDA engine cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import build as _build
+from .layout import INDEX_TYPES
+
+_LIB_PATH = _build.LIB
+_lib = None
+
+PDXG_OK = 0
+PDXG_ERR_INVALID_ARGUMENT = 1
+PDXG_QUERY_TRANSFORMED = 1
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+def library() -> C.CDLL:
+    """Loads (building first if missing or stale) the engine library."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or _build._stale():
+            _build.build()
+        lib = C.CDLL(_LIB_PATH)
+        vp = C.c_void_p
+
+        def fn(name, res, *args):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = list(args)
+
+        fn("pdxg_last_error", C.c_char_p)
+        fn("pdxg_load", C.c_int, C.c_char_p, C.c_int, C.POINTER(vp))
+        fn("pdxg_load_buffer", C.c_int, C.c_char_p, C.c_uint64, C.c_int, C.POINTER(vp))
+        fn("pdxg_free", None, vp)
+        fn("pdxg_set_nprobe", C.c_int, vp, C.c_uint32)
+        fn("pdxg_set_pruning_aggressiveness", C.c_int, vp, C.c_float)
+        fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
+        fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
+        fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
+        fn("pdxg_search_with_order", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u32p, C.c_uint32,
+           C.c_uint32, _u32p, _f32p, _u32p)
+        fn("pdxg_filtered_search", C.c_int, vp, _f32p, C.c_uint32, _u64p, C.c_uint64, C.c_uint32,
+           _u32p, _f32p, _u32p)
+        fn("pdxg_filtered_search_batch", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u64p, _u64p,
+           C.c_uint32, _u32p, _f32p, _u32p)
+        fn("pdxg_save", C.c_int, vp, C.c_char_p)
+        fn("pdxg_index_type", C.c_int, vp)
+        fn("pdxg_num_dimensions", C.c_uint32, vp)
+        fn("pdxg_num_clusters", C.c_uint32, vp)
+        fn("pdxg_nprobe", C.c_uint32, vp)
+        fn("pdxg_cluster_size", C.c_uint32, vp, C.c_uint32)
+        fn("pdxg_cluster_row_ids", C.c_int, vp, C.c_uint32, _u32p, C.c_uint32)
+        fn("pdxg_in_memory_size_in_bytes", C.c_uint64, vp)
+        fn("pdxg_num_embeddings", C.c_uint64, vp)
+        fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != PDXG_OK:
+        msg = library().pdxg_last_error().decode(errors="replace")
+        if rc == PDXG_ERR_INVALID_ARGUMENT:
+            raise ValueError(msg)
+        raise RuntimeError(msg)
+
+
+class Handle:
+    """Owns one pdxg_index*."""
+
+    def __init__(self, ptr: int):
+        self.ptr = C.c_void_p(ptr)
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and self.ptr.value and _lib is not None:
+            _lib.pdxg_free(self.ptr)
+            self.ptr = C.c_void_p(0)
+
+
+def _load_handle(path: Optional[str] = None, data: Optional[bytes] = None, device: int = 0) -> Handle:
+    lib = library()
+    out = C.c_void_p()
+    if path is not None:
+        _check(lib.pdxg_load(os.fsencode(path), device, C.byref(out)))
+    else:
+        _check(lib.pdxg_load_buffer(data, len(data), device, C.byref(out)))
+    return Handle(out.value)
+
+
+_METRICS = {0: "l2sq", 1: "cosine", 2: "ip"}
+
+
+class PDXIndex:
+    """GPU-resident PDX index with the reference's `compiled.PDXIndex` interface."""
+
+    def __init__(self, index_type: str, num_dimensions: int, distance_metric: int = 0, seed: int = 42,
+                 num_clusters: int = 0, num_meso_clusters: int = 0, normalize: bool = False,
+                 sampling_fraction: float = 0.0, kmeans_iters: int = 10,
+                 hierarchical_indexing: bool = True, n_threads: int = 0, device: int = 0):
+        if index_type not in INDEX_TYPES:
+            raise RuntimeError(f"Unknown index type: {index_type}. Valid types: pdx_f32, pdx_u8, "
+                               "pdx_tree_f32, pdx_tree_u8")
+        if distance_metric not in _METRICS:
+            raise RuntimeError(f"Unknown distance metric: {distance_metric}")
+        # PDXIndexConfig::Validate (index.hpp:39-62)
+        if num_dimensions == 0 or num_dimensions > 16384:
+            raise ValueError(f"num_dimensions must be between 1 and 16384, got {num_dimensions}")
+        if sampling_fraction < 0.0 or sampling_fraction > 1.0:
+            raise ValueError(f"sampling_fraction must be between 0.0 and 1.0, got {sampling_fraction}")
+        if num_meso_clusters > 0 and num_clusters > 0 and num_meso_clusters >= num_clusters:
+            raise ValueError(f"num_meso_clusters ({num_meso_clusters}) must be smaller than "
+                             f"num_clusters ({num_clusters})")
+        if kmeans_iters == 0 or kmeans_iters >= 100:
+            raise ValueError(f"kmeans_iters must be between 1 and 99, got {kmeans_iters}")
+        self._type = index_type
+        self._d = num_dimensions
+        self._metric = distance_metric
+        self._seed = seed
+        self._num_clusters = num_clusters
+        self._num_meso = num_meso_clusters
+        self._normalize = normalize or distance_metric in (1, 2)
+        self._kmeans_iters = kmeans_iters
+        self._device = device
+        self._nprobe = 0
+        self._h: Optional[Handle] = None
+
+    # -- construction --------------------------------------------------------------------
+    @classmethod
+    def _from_handle(cls, h: Handle) -> "PDXIndex":
+        self = cls.__new__(cls)
+        lib = library()
+        t = lib.pdxg_index_type(h.ptr)
+        self._type = {v: k for k, v in INDEX_TYPES.items()}[t]
+        self._d = lib.pdxg_num_dimensions(h.ptr)
+        self._metric = 0
+        self._seed = 42
+        self._num_clusters = lib.pdxg_num_clusters(h.ptr)
+        self._num_meso = 0
+        self._normalize = False
+        self._kmeans_iters = 10
+        self._device = 0
+        self._nprobe = 0
+        self._h = h
+        return self
+
+    def build_index(self, data: np.ndarray) -> None:
+        from .builder import build_index as _build_index
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        if data.ndim != 2:
+            raise RuntimeError("data must be a 2D numpy array (n_embeddings x dimensions)")
+        if data.shape[1] != self._d:
+            raise ValueError(f"data has {data.shape[1]} dimensions, index expects {self._d}")
+        dev = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                dev = f"cuda:{self._device}"
+        except Exception:
+            dev = None
+        f = _build_index(data, self._type, num_clusters=self._num_clusters,
+                         num_meso_clusters=self._num_meso, normalize=self._normalize,
+                         seed=self._seed, kmeans_iters=self._kmeans_iters, device=dev)
+        self._h = _load_handle(data=f.to_bytes(), device=self._device)
+        _check(library().pdxg_set_nprobe(self._h.ptr, self._nprobe))
+
+    def _handle(self) -> Handle:
+        if self._h is None:
+            raise RuntimeError("index is empty: call build_index() or load_index() first")
+        return self._h
+
+    # -- search ----------------------------------------------------------------------------
+    def set_nprobe(self, nprobe: int) -> None:
+        self._nprobe = int(nprobe)
+        if self._h is not None:
+            _check(library().pdxg_set_nprobe(self._h.ptr, self._nprobe))
+
+    def search(self, query: np.ndarray, knn: int) -> Tuple[np.ndarray, np.ndarray]:
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        if q.ndim != 1:
+            raise RuntimeError("query must be a 1D numpy array")
+        ids, ds, cnt = self.search_batch(q[None, :], knn)
+        return ids[0, :cnt[0]].copy(), ds[0, :cnt[0]].copy()
+
+    def search_batch(self, queries: np.ndarray, knn: int, transformed: bool = False):
+        """Batched search (extension): returns ids [nq, k], distances [nq, k], counts [nq]."""
+        h = self._handle()
+        Q = np.ascontiguousarray(queries, dtype=np.float32)
+        if Q.ndim != 2 or Q.shape[1] != self.get_num_dimensions():
+            raise ValueError("queries must be a 2D array (n_queries x num_dimensions)")
+        nq = Q.shape[0]
+        ids = np.empty((nq, knn), np.uint32)
+        ds = np.empty((nq, knn), np.float32)
+        cnt = np.empty(nq, np.uint32)
+        _check(library().pdxg_search(h.ptr, Q.ctypes.data, nq, knn,
+                                     PDXG_QUERY_TRANSFORMED if transformed else 0,
+                                     ids.ctypes.data, ds.ctypes.data, cnt.ctypes.data))
+        return ids, ds, cnt
+
+    def search_with_order(self, queries: np.ndarray, knn: int, order, transformed: bool = False):
+        """PDXearch::SetClusterAccessOrder + Search (searcher.hpp:48-54), batched."""
+        h = self._handle()
+        Q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        o = np.ascontiguousarray(order, dtype=np.uint32)
+        nq = Q.shape[0]
+        ids = np.empty((nq, knn), np.uint32)
+        ds = np.empty((nq, knn), np.float32)
+        cnt = np.empty(nq, np.uint32)
+        _check(library().pdxg_search_with_order(h.ptr, Q, nq, knn, o, len(o),
+                                                PDXG_QUERY_TRANSFORMED if transformed else 0,
+                                                ids, ds, cnt))
+        return ids, ds, cnt
+
+    def filtered_search(self, query: np.ndarray, knn: int, row_ids: np.ndarray):
+        h = self._handle()
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        if q.ndim != 1:
+            raise RuntimeError("query must be a 1D numpy array")
+        r = np.ascontiguousarray(row_ids, dtype=np.uint64)
+        if r.ndim != 1:
+            raise RuntimeError("row_ids must be a 1D numpy array")
+        ids = np.empty(knn, np.uint32)
+        ds = np.empty(knn, np.float32)
+        cnt = np.zeros(1, np.uint32)
+        _check(library().pdxg_filtered_search(h.ptr, q, knn, r, len(r), 0, ids, ds, cnt))
+        return ids[:cnt[0]].copy(), ds[:cnt[0]].copy()
+
+    def filtered_search_batch(self, queries: np.ndarray, knn: int, row_id_lists, transformed=False):
+        """Batched filtered search (extension): row_id_lists[i] is None (unfiltered) or ids."""
+        h = self._handle()
+        Q = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = Q.shape[0]
+        offsets = np.zeros(nq + 1, np.uint64)
+        parts = []
+        pos = 0
+        for i, lst in enumerate(row_id_lists):
+            if lst is None:
+                offsets[i] = np.uint64(np.iinfo(np.uint64).max)
+            else:
+                a = np.asarray(lst, dtype=np.uint64)
+                offsets[i] = pos
+                parts.append(a)
+                pos += len(a)
+        offsets[nq] = pos
+        # unfiltered queries need the next filtered start as their successor's bound
+        rows = np.concatenate(parts) if parts else np.zeros(1, np.uint64)
+        ids = np.empty((nq, knn), np.uint32)
+        ds = np.empty((nq, knn), np.float32)
+        cnt = np.empty(nq, np.uint32)
+        _check(library().pdxg_filtered_search_batch(h.ptr, Q, nq, knn, rows, offsets,
+                                                    PDXG_QUERY_TRANSFORMED if transformed else 0,
+                                                    ids, ds, cnt))
+        return ids, ds, cnt
+
+    def prepare_queries(self, queries: np.ndarray) -> np.ndarray:
+        """Normalized (if the index is) and rotated queries as the engine searches them."""
+        h = self._handle()
+        Q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        out = np.empty_like(Q)
+        _check(library().pdxg_prepare_queries(h.ptr, Q, Q.shape[0], out))
+        return out
+
+    def set_pruning_aggressiveness(self, epsilon0: float) -> None:
+        _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))
+
+    def set_threads_per_query(self, threads: int) -> None:
+        _check(library().pdxg_set_threads_per_query(self._handle().ptr, int(threads)))
+
+    # -- persistence & getters -----------------------------------------------------------
+    def save(self, path: str) -> None:
+        _check(library().pdxg_save(self._handle().ptr, os.fsencode(path)))
+
+    def get_num_dimensions(self) -> int:
+        return library().pdxg_num_dimensions(self._handle().ptr) if self._h else self._d
+
+    def get_num_clusters(self) -> int:
+        return library().pdxg_num_clusters(self._handle().ptr)
+
+    def get_cluster_size(self, cluster_id: int) -> int:
+        if cluster_id >= self.get_num_clusters():
+            raise ValueError("cluster_id out of range")
+        return library().pdxg_cluster_size(self._handle().ptr, cluster_id)
+
+    def get_cluster_row_ids(self, cluster_id: int) -> np.ndarray:
+        n = self.get_cluster_size(cluster_id)
+        out = np.empty(max(n, 1), np.uint32)
+        _check(library().pdxg_cluster_row_ids(self._handle().ptr, cluster_id, out, len(out)))
+        return out[:n].copy()
+
+    def get_in_memory_size_in_bytes(self) -> int:
+        return int(library().pdxg_in_memory_size_in_bytes(self._handle().ptr))
+
+    def get_num_embeddings(self) -> int:
+        return int(library().pdxg_num_embeddings(self._handle().ptr))
+
+    @property
+    def handle(self) -> Handle:
+        return self._handle()
+
+    # -- maintenance (tree indexes in the reference) -----------------------------------
+    def append(self, row_id: int, embedding: np.ndarray) -> None:
+        if self._type in ("pdx_f32", "pdx_u8"):
+            raise RuntimeError("Append is not implemented in PDXIndex. Use PDXTreeIndex instead.")
+        raise RuntimeError("Append is not supported by the GPU engine yet")
+
+    def delete(self, row_id: int) -> None:
+        if self._type in ("pdx_f32", "pdx_u8"):
+            raise RuntimeError("Delete is not implemented in PDXIndex. Use PDXTreeIndex instead.")
+        raise RuntimeError("Delete is not supported by the GPU engine yet")
+
+
+def load_index(path: str, device: int = 0) -> PDXIndex:
+    """Load a PDX index from a single file (auto-detects type)."""
+    return PDXIndex._from_handle(_load_handle(path=path, device=device))

@@ -1,0 +1,78 @@
+// Shared definitions of the B200 PDX search engine: the device-resident index layout and the
+// kernel parameter blocks. Host and device code both include this header.
+//
+// Device layout of one cluster (all offsets in bytes from the arena base, 256-byte aligned):
+//   vertical block   : n_vwords rows x n_pad 32-bit words. F32: one row per vertical dimension
+//                      (dim-major, consecutive vectors in consecutive words). U8: one row per
+//                      group of 4 vertical dimensions, each word holding the 4 interleaved bytes
+//                      of one vector (the reference's U8_INTERLEAVE_SIZE packing); a trailing
+//                      group of d_v % 4 dims is zero-padded to a full word.
+//   horizontal blocks: n_hblocks x n_pad rows of 64 elements (F32: 256 B rows, U8: 64 B rows),
+//                      the reference's 64-dim row-major sub-blocks.
+//   row ids          : n u32.
+// n_pad rounds the cluster size up to 32 so every dimension row starts on a 128-byte line.
+#pragma once
+#include <cstdint>
+
+namespace pdxg {
+
+constexpr int kHDim = 64;               // H_DIM_SIZE (common.hpp:45)
+constexpr int kMaxDims = 16384;         // PDX_MAX_DIMS (common.hpp:44)
+constexpr int kNumFetchSizes = 20;      // DIMENSIONS_FETCHING_SIZES (common.hpp:47-49)
+constexpr float kSelectivity = 0.80f;   // selectivity_threshold (searcher.hpp:57)
+
+struct DevCluster {
+    uint64_t vert_off;  // vertical block
+    uint64_t hor_off;   // horizontal blocks
+    uint64_t ids_off;   // row ids
+    uint32_t n;         // vectors in the cluster (used capacity)
+    uint32_t n_pad;     // row stride in vectors (multiple of 32)
+    uint32_t sel_word;  // first 32-bit word of this cluster in a filter selection bitmap
+    uint32_t pad_;
+};
+
+struct DevLevel {
+    const DevCluster* clusters;  // [nclusters]
+    const float* centroids;      // [nclusters x d] f32 (rotated space)
+    uint32_t nclusters;
+    uint32_t d, dv, dh;
+    uint32_t n_vwords;           // vertical words per vector: F32 dv, U8 ceil(dv / 4)
+    uint32_t qw_hoff;            // U8: first horizontal word of the packed query (16B aligned)
+    uint32_t n_hblocks;          // dh / 64
+    uint32_t max_n;              // largest cluster
+    uint32_t is_u8;
+    uint32_t sel_words;          // words of one selection bitmap over this level
+    float scale_sq;              // U8: quantization_scale^2
+    float inv_scale_sq;          // U8: 1 / quantization_scale^2
+    float base, scale;           // U8 quantization parameters
+};
+
+// One batched search launch.
+struct SearchParams {
+    const uint8_t* arena;
+    DevLevel l1;                 // data clusters
+    DevLevel l0;                 // meso clusters (tree indexes only)
+    int is_tree;
+    const float* ratios;         // ADSampling ratio table [d] (adsampling.hpp:147-157)
+    const float* queries;        // prepared (normalized + rotated) queries [nq x d]
+    uint32_t nq;
+    uint32_t k;
+    uint32_t nprobe;             // L1 clusters to visit (already resolved: 1..nclusters)
+    uint32_t top_nprobe;         // tree: meso clusters probed by the top-level search
+    const uint32_t* order;       // optional caller cluster order [n_order] shared by all queries
+    uint32_t n_order;
+    const uint32_t* sel_bits;    // optional: [n_filters x l1.sel_words] selection bitmaps
+    const uint32_t* passing;     // optional: [n_filters x l1.nclusters] passing counts
+    const int32_t* filter_of;    // optional: [nq] filter slot per query, -1 = unfiltered
+    uint32_t* out_ids;           // [nq x k]
+    float* out_dists;            // [nq x k]
+    uint32_t* out_counts;        // [nq]
+    uint32_t* queue;             // work counter (zeroed before launch)
+    // shared-memory carve-up (bytes), computed by the host
+    uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_total;
+    uint32_t work_cap;           // entries of the dist / pos work arrays (power of two)
+    uint32_t heap_cap;           // entries of the heap arrays (power of two)
+    uint32_t order_cap;          // entries of the cluster order list
+};
+
+}  // namespace pdxg

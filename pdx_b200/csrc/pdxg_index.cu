@@ -1,0 +1,978 @@
+// Host side of the B200 PDX engine: index-file parsing, the device arena, workspaces and the
+// C ABI declared in include/pdx_b200.h.
+//
+// Loading follows LoadPDXIndex / Restore (index.hpp:1736-1760, 242-267, 516-543) and
+// IVF::Load / IVFTree::Load (ivf_wrapper.hpp:89-131, 218-312) for the byte layout, then
+// re-lays every cluster into the device format described in pdxg_common.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pdx_b200.h"
+#include "pdxg_common.cuh"
+
+namespace pdxg {
+cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid, cudaStream_t st);
+int search_occupancy(bool u8, int threads, size_t smem);
+cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, const float* rotation,
+                                   bool normalize, float* norms_ws, float* out, cudaStream_t st);
+}  // namespace pdxg
+
+using namespace pdxg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define PDXG_CUDA(x)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (x);                                                             \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(PDXG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+uint32_t next_pow2(uint32_t x) {
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+// ADSamplingPruner::GetRatio (adsampling.hpp:147-157), same types and operation order.
+float adsampling_ratio(const size_t& visited, uint32_t d, float eps0) {
+    if (visited == 0) return 1;
+    if (visited == d) return 1.0;
+    return static_cast<float>(visited) / d * (1.0 + eps0 / std::sqrt(visited)) *
+           (1.0 + eps0 / std::sqrt(visited));
+}
+
+void dimension_split(uint32_t d, uint32_t& h, uint32_t& v) {  // common.hpp:133-159
+    float prop = 0.75f;
+    if (d <= 128) prop = 0.25f;
+    h = static_cast<uint32_t>(static_cast<float>(d) * prop);
+    v = d - h;
+    if (h % kHDim > 0) {
+        h = ((h + kHDim / 2) / kHDim) * kHDim;
+        v = d - h;
+    }
+    if (!v) {
+        h = kHDim;
+        v = d - h;
+    }
+    if (d <= kHDim) {
+        h = 0;
+        v = d;
+    }
+}
+
+struct Cursor {
+    const uint8_t* p;
+    const uint8_t* end;
+    bool ok = true;
+    bool need(uint64_t n) {
+        if (!ok || (uint64_t)(end - p) < n) ok = false;
+        return ok;
+    }
+    uint32_t u32() {
+        uint32_t v = 0;
+        if (need(4)) {
+            std::memcpy(&v, p, 4);
+            p += 4;
+        }
+        return v;
+    }
+    uint8_t u8() {
+        uint8_t v = 0;
+        if (need(1)) v = *p++;
+        return v;
+    }
+    float f32() {
+        float v = 0;
+        if (need(4)) {
+            std::memcpy(&v, p, 4);
+            p += 4;
+        }
+        return v;
+    }
+    const uint8_t* take(uint64_t n) {
+        if (!need(n)) return nullptr;
+        const uint8_t* r = p;
+        p += n;
+        return r;
+    }
+};
+
+struct FileCluster {
+    uint32_t n = 0, max_cap = 0;
+    const uint8_t* data = nullptr;  // compact PDX block inside the file buffer
+    const uint8_t* ids = nullptr;   // u32[n]
+};
+
+struct HostLevel {
+    bool u8 = false;
+    uint32_t d = 0, dv = 0, dh = 0;
+    std::vector<FileCluster> fc;
+    std::vector<DevCluster> meta;
+    std::vector<uint32_t> n, max_cap;
+    std::vector<uint64_t> ids_start;
+    std::vector<uint32_t> ids;  // host copy of all row ids, cluster after cluster
+    std::vector<float> centroids;
+    uint32_t max_n = 0, sel_words = 0, n_vwords = 0, qw_hoff = 0, n_hblocks = 0;
+    uint64_t total_vectors = 0;
+};
+
+bool read_level(Cursor& c, HostLevel& lv, uint32_t ncl) {
+    lv.fc.resize(ncl);
+    for (uint32_t i = 0; i < ncl; ++i) {
+        lv.fc[i].n = c.u32();
+        lv.fc[i].max_cap = c.u32();
+    }
+    if (!c.ok) return false;
+    const uint64_t esz = lv.u8 ? 1 : 4;
+    for (uint32_t i = 0; i < ncl; ++i) {
+        lv.fc[i].data = c.take((uint64_t)lv.fc[i].n * lv.d * esz);
+        if (!c.ok) return false;
+    }
+    for (uint32_t i = 0; i < ncl; ++i) {
+        lv.fc[i].ids = c.take((uint64_t)lv.fc[i].n * 4);
+        if (!c.ok) return false;
+    }
+    return true;
+}
+
+// Byte layout of the level's clusters inside the arena, starting at `off`.
+uint64_t plan_level(HostLevel& lv, uint64_t off) {
+    lv.n_vwords = lv.u8 ? (lv.dv + 3) / 4 : lv.dv;
+    lv.qw_hoff = (lv.n_vwords + 3) / 4 * 4;
+    lv.n_hblocks = lv.dh / kHDim;
+    const uint64_t esz = lv.u8 ? 1 : 4;
+    const size_t ncl = lv.fc.size();
+    lv.meta.resize(ncl);
+    lv.n.resize(ncl);
+    lv.max_cap.resize(ncl);
+    lv.ids_start.resize(ncl + 1);
+    lv.max_n = 0;
+    lv.total_vectors = 0;
+    uint32_t sel = 0;
+    for (size_t i = 0; i < ncl; ++i) {
+        const uint32_t n = lv.fc[i].n;
+        const uint32_t n_pad = std::max<uint32_t>(32, (n + 31) / 32 * 32);
+        DevCluster& m = lv.meta[i];
+        m.n = n;
+        m.n_pad = n_pad;
+        m.sel_word = sel;
+        m.pad_ = 0;
+        sel += n_pad / 32;
+        off = align_up(off, 256);
+        m.vert_off = off;
+        off += (uint64_t)lv.n_vwords * n_pad * 4;
+        off = align_up(off, 256);
+        m.hor_off = off;
+        off += (uint64_t)lv.n_hblocks * n_pad * kHDim * esz;
+        off = align_up(off, 256);
+        m.ids_off = off;
+        off += (uint64_t)n_pad * 4;
+        lv.n[i] = n;
+        lv.max_cap[i] = lv.fc[i].max_cap;
+        lv.ids_start[i] = lv.total_vectors;
+        lv.total_vectors += n;
+        lv.max_n = std::max(lv.max_n, n);
+    }
+    lv.ids_start[ncl] = lv.total_vectors;
+    lv.sel_words = sel;
+    return align_up(off, 256);
+}
+
+// Fills the staging image of the arena for one level (compact file block -> device layout).
+void fill_level(HostLevel& lv, uint8_t* img) {
+    const uint32_t dv = lv.dv;
+    lv.ids.resize(lv.total_vectors);
+    for (size_t i = 0; i < lv.fc.size(); ++i) {
+        const FileCluster& f = lv.fc[i];
+        const DevCluster& m = lv.meta[i];
+        const uint64_t n = f.n, np = m.n_pad;
+        if (!lv.u8) {
+            for (uint32_t j = 0; j < dv; ++j)
+                std::memcpy(img + m.vert_off + (uint64_t)j * np * 4, f.data + (uint64_t)j * n * 4, n * 4);
+            const uint8_t* hsrc = f.data + (uint64_t)dv * n * 4;
+            for (uint32_t b = 0; b < lv.n_hblocks; ++b)
+                std::memcpy(img + m.hor_off + (uint64_t)b * np * kHDim * 4,
+                            hsrc + (uint64_t)b * n * kHDim * 4, n * kHDim * 4);
+        } else {
+            const uint32_t full = dv / 4, rem = dv % 4;
+            for (uint32_t g = 0; g < full; ++g)
+                std::memcpy(img + m.vert_off + (uint64_t)g * np * 4, f.data + (uint64_t)g * n * 4, n * 4);
+            if (rem) {
+                const uint8_t* src = f.data + (uint64_t)full * n * 4;
+                uint8_t* dst = img + m.vert_off + (uint64_t)full * np * 4;
+                for (uint64_t v = 0; v < n; ++v)
+                    for (uint32_t t = 0; t < rem; ++t) dst[v * 4 + t] = src[v * rem + t];
+            }
+            const uint8_t* hsrc = f.data + (uint64_t)dv * n;
+            for (uint32_t b = 0; b < lv.n_hblocks; ++b)
+                std::memcpy(img + m.hor_off + (uint64_t)b * np * kHDim, hsrc + (uint64_t)b * n * kHDim,
+                            n * kHDim);
+        }
+        std::memcpy(img + m.ids_off, f.ids, n * 4);
+        std::memcpy(lv.ids.data() + lv.ids_start[i], f.ids, n * 4);
+    }
+}
+
+struct Workspace {
+    uint32_t q_cap = 0, k_cap = 0;
+    float* d_q = nullptr;
+    float* d_rq = nullptr;
+    float* d_norms = nullptr;
+    uint32_t* d_ids = nullptr;
+    float* d_dists = nullptr;
+    uint32_t* d_counts = nullptr;
+    uint32_t* d_queue = nullptr;
+    uint32_t* d_order = nullptr;
+    uint32_t order_cap = 0;
+    uint32_t* d_sel = nullptr;
+    uint64_t sel_cap = 0;
+    uint32_t* d_pass = nullptr;
+    uint64_t pass_cap = 0;
+    int32_t* d_filter_of = nullptr;
+    uint32_t fo_cap = 0;
+};
+
+}  // namespace
+
+struct pdxg_index {
+    int device = 0;
+    int type = 0;
+    uint32_t d = 0, dv = 0, dh = 0;
+    bool tree = false, u8 = false, normalized = false;
+    float base = 0.0f, scale = 1.0f;
+    uint32_t rot_rows = 0, rot_cols = 0;
+    std::vector<float> rotation;
+    HostLevel l1, l0;
+    uint8_t* arena = nullptr;
+    uint64_t arena_bytes = 0;
+    DevCluster* d_cl1 = nullptr;
+    DevCluster* d_cl0 = nullptr;
+    float* d_cent1 = nullptr;
+    float* d_cent0 = nullptr;
+    float* d_rot = nullptr;
+    float* d_ratios = nullptr;
+    float eps0 = 1.5f;
+    uint32_t nprobe = 0;
+    uint32_t threads = 0;
+    int num_sms = 0;
+    size_t max_smem = 0;
+    std::vector<uint32_t> rid_cluster, rid_pos;
+    cudaStream_t stream = nullptr;
+    Workspace ws;
+    std::mutex mu;
+};
+
+namespace {
+
+template <class T>
+int dev_grow(T*& ptr, uint64_t& cap, uint64_t need) {
+    if (need <= cap && ptr) return PDXG_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    const uint64_t n = std::max<uint64_t>(need, 1);
+    PDXG_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+    cap = n;
+    return PDXG_OK;
+}
+
+int upload_ratios(pdxg_index* ix) {
+    std::vector<float> r(ix->d);
+    for (size_t i = 0; i < ix->d; ++i) r[i] = adsampling_ratio(i, ix->d, ix->eps0);
+    PDXG_CUDA(cudaMemcpy(ix->d_ratios, r.data(), sizeof(float) * ix->d, cudaMemcpyHostToDevice));
+    return PDXG_OK;
+}
+
+DevLevel make_level(const HostLevel& lv, const DevCluster* dcl, const float* cent, float base,
+                    float scale) {
+    DevLevel L{};
+    L.clusters = dcl;
+    L.centroids = cent;
+    L.nclusters = (uint32_t)lv.fc.size();
+    L.d = lv.d;
+    L.dv = lv.dv;
+    L.dh = lv.dh;
+    L.n_vwords = lv.n_vwords;
+    L.qw_hoff = lv.qw_hoff;
+    L.n_hblocks = lv.n_hblocks;
+    L.max_n = lv.max_n;
+    L.is_u8 = lv.u8 ? 1 : 0;
+    L.sel_words = lv.sel_words;
+    L.base = base;
+    L.scale = scale;
+    L.scale_sq = scale * scale;
+    L.inv_scale_sq = 1.0f / L.scale_sq;
+    return L;
+}
+
+void free_index(pdxg_index* ix) {
+    if (!ix) return;
+    cudaSetDevice(ix->device);
+    cudaFree(ix->arena);
+    cudaFree(ix->d_cl1);
+    cudaFree(ix->d_cl0);
+    cudaFree(ix->d_cent1);
+    cudaFree(ix->d_cent0);
+    cudaFree(ix->d_rot);
+    cudaFree(ix->d_ratios);
+    Workspace& w = ix->ws;
+    cudaFree(w.d_q);
+    cudaFree(w.d_rq);
+    cudaFree(w.d_norms);
+    cudaFree(w.d_ids);
+    cudaFree(w.d_dists);
+    cudaFree(w.d_counts);
+    cudaFree(w.d_queue);
+    cudaFree(w.d_order);
+    cudaFree(w.d_sel);
+    cudaFree(w.d_pass);
+    cudaFree(w.d_filter_of);
+    if (ix->stream) cudaStreamDestroy(ix->stream);
+    delete ix;
+}
+
+int load_from_bytes(const uint8_t* buf, uint64_t size, int device, pdxg_index** out) {
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    Cursor c{buf, buf + size};
+    const uint8_t type = c.u8();
+    if (!c.ok) return fail(PDXG_ERR_FORMAT, "index file is empty");
+    if (type > 3) return fail(PDXG_ERR_FORMAT, "Unknown PDX index type: " + std::to_string(type));
+    auto* ix = new pdxg_index();
+    ix->device = device;
+    ix->type = type;
+    ix->tree = type >= 2;
+    ix->u8 = (type == 1 || type == 3);
+    ix->rot_rows = c.u32();
+    ix->rot_cols = c.u32();
+    const uint8_t* rot = c.take((uint64_t)ix->rot_rows * ix->rot_cols * 4);
+    uint32_t d = c.u32(), dv = c.u32(), dh = c.u32();
+    if (!c.ok) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "truncated index header");
+    }
+    uint32_t eh = 0, ev = 0;
+    if (d == 0 || d > (uint32_t)kMaxDims) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "num_dimensions out of range: " + std::to_string(d));
+    }
+    dimension_split(d, eh, ev);
+    if (dv != ev || dh != eh) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "dimension split in file does not match GetPDXDimensionSplit");
+    }
+    if (ix->rot_rows == 1 && ix->rot_cols == d) {
+        free_index(ix);
+        return fail(PDXG_ERR_UNSUPPORTED,
+                    "index uses the DCT rotation (1 x d sign vector); not supported by this engine");
+    }
+    if (ix->rot_rows != d || ix->rot_cols != d) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "rotation matrix shape does not match num_dimensions");
+    }
+    ix->d = d;
+    ix->dv = dv;
+    ix->dh = dh;
+    ix->rotation.resize((size_t)d * d);
+    std::memcpy(ix->rotation.data(), rot, (size_t)d * d * 4);
+    for (HostLevel* lv : {&ix->l1, &ix->l0}) {
+        lv->d = d;
+        lv->dv = dv;
+        lv->dh = dh;
+    }
+    ix->l1.u8 = ix->u8;
+    ix->l0.u8 = false;
+    bool ok;
+    uint32_t n1, n0 = 0;
+    if (!ix->tree) {
+        n1 = c.u32();
+        ok = c.ok && read_level(c, ix->l1, n1);
+    } else {
+        n1 = c.u32();
+        n0 = c.u32();
+        ok = c.ok && read_level(c, ix->l0, n0) && read_level(c, ix->l1, n1);
+    }
+    if (!ok) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "truncated index payload");
+    }
+    ix->normalized = c.u8() != 0;
+    const uint32_t ncent = ix->tree ? n0 : n1;
+    const uint8_t* cent = c.take((uint64_t)ncent * d * 4);
+    if (ix->u8) {
+        ix->base = c.f32();
+        ix->scale = c.f32();
+    }
+    if (!c.ok) {
+        free_index(ix);
+        return fail(PDXG_ERR_FORMAT, "truncated index trailer");
+    }
+    if (ix->tree) {
+        ix->l0.centroids.assign(reinterpret_cast<const float*>(cent),
+                                reinterpret_cast<const float*>(cent) + (size_t)n0 * d);
+        // L1 centroids are the vectors of the L0 clusters (IVFTree::Save does not store them).
+        ix->l1.centroids.assign((size_t)n1 * d, 0.0f);
+        for (const FileCluster& f : ix->l0.fc) {
+            const float* data = reinterpret_cast<const float*>(f.data);
+            for (uint32_t p = 0; p < f.n; ++p) {
+                uint32_t id;
+                std::memcpy(&id, f.ids + (size_t)p * 4, 4);
+                if (id >= n1) {
+                    free_index(ix);
+                    return fail(PDXG_ERR_FORMAT, "meso cluster references an unknown cluster");
+                }
+                float* dst = ix->l1.centroids.data() + (size_t)id * d;
+                for (uint32_t j = 0; j < dv; ++j) dst[j] = data[(size_t)j * f.n + p];
+                for (uint32_t b = 0; b < dh; b += kHDim)
+                    std::memcpy(dst + dv + b, data + (size_t)dv * f.n + (size_t)b * f.n + (size_t)p * kHDim,
+                                kHDim * 4);
+            }
+        }
+    } else {
+        ix->l1.centroids.assign(reinterpret_cast<const float*>(cent),
+                                reinterpret_cast<const float*>(cent) + (size_t)n1 * d);
+    }
+
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        free_index(ix);
+        return fail(PDXG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    cudaDeviceGetAttribute(&ix->num_sms, cudaDevAttrMultiProcessorCount, device);
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    ix->max_smem = (size_t)smem_optin;
+
+    uint64_t off = plan_level(ix->l1, 0);
+    if (ix->tree) {
+        for (DevCluster& m : ix->l0.meta) (void)m;
+        const uint64_t start0 = off;
+        off = plan_level(ix->l0, start0);
+    }
+    ix->arena_bytes = off;
+    std::vector<uint8_t> img(off, 0);
+    fill_level(ix->l1, img.data());
+    if (ix->tree) fill_level(ix->l0, img.data());
+
+    int rc = PDXG_OK;
+    auto step = [&](cudaError_t err, const char* what) {
+        if (rc == PDXG_OK && err != cudaSuccess)
+            rc = fail(PDXG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+    };
+    step(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    step(cudaMalloc(&ix->arena, std::max<uint64_t>(off, 256)), "cudaMalloc(arena)");
+    if (rc == PDXG_OK)
+        step(cudaMemcpy(ix->arena, img.data(), off, cudaMemcpyHostToDevice), "cudaMemcpy(arena)");
+    img.clear();
+    img.shrink_to_fit();
+    auto upload = [&](auto*& dptr, const auto& vec, const char* what) {
+        using T = typename std::decay<decltype(vec)>::type::value_type;
+        if (rc != PDXG_OK) return;
+        step(cudaMalloc(&dptr, std::max<size_t>(vec.size(), 1) * sizeof(T)), what);
+        if (rc == PDXG_OK && !vec.empty())
+            step(cudaMemcpy(dptr, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice), what);
+    };
+    upload(ix->d_cl1, ix->l1.meta, "clusters");
+    upload(ix->d_cent1, ix->l1.centroids, "centroids");
+    if (ix->tree) {
+        upload(ix->d_cl0, ix->l0.meta, "meso clusters");
+        upload(ix->d_cent0, ix->l0.centroids, "meso centroids");
+    }
+    upload(ix->d_rot, ix->rotation, "rotation");
+    if (rc == PDXG_OK) step(cudaMalloc(&ix->d_ratios, sizeof(float) * d), "ratios");
+    if (rc == PDXG_OK) rc = upload_ratios(ix);
+    if (rc != PDXG_OK) {
+        free_index(ix);
+        return rc;
+    }
+    // row id -> (cluster, position), as BuildRowIdClusterMapping (index.hpp:421-433)
+    const uint64_t total = ix->l1.total_vectors;
+    ix->rid_cluster.assign(total, 0xFFFFFFFFu);
+    ix->rid_pos.assign(total, 0);
+    for (size_t ci = 0; ci < ix->l1.fc.size(); ++ci)
+        for (uint32_t p = 0; p < ix->l1.n[ci]; ++p) {
+            const uint32_t rid = ix->l1.ids[ix->l1.ids_start[ci] + p];
+            if (rid < total) {
+                ix->rid_cluster[rid] = (uint32_t)ci;
+                ix->rid_pos[rid] = p;
+            }
+        }
+    // file buffer pointers are not kept
+    for (HostLevel* lv : {&ix->l1, &ix->l0})
+        for (FileCluster& f : lv->fc) {
+            f.data = nullptr;
+            f.ids = nullptr;
+        }
+    *out = ix;
+    return PDXG_OK;
+}
+
+struct Launch {
+    SearchParams p{};
+    bool u8 = false;
+    int threads = 256;
+    int grid = 1;
+};
+
+int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
+                Launch& L) {
+    SearchParams& p = L.p;
+    p.arena = ix->arena;
+    p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale);
+    p.is_tree = ix->tree ? 1 : 0;
+    if (ix->tree) p.l0 = make_level(ix->l0, ix->d_cl0, ix->d_cent0, 0.0f, 1.0f);
+    p.ratios = ix->d_ratios;
+    p.nq = nq;
+    p.k = k;
+    const uint32_t n1 = p.l1.nclusters;
+    // flat: searcher.hpp:614-616; tree: index.hpp:546-556
+    const uint32_t np_flat = (ix->nprobe == 0 || ix->nprobe > n1) ? n1 : ix->nprobe;
+    uint32_t top = 0;
+    if (ix->tree) {
+        top = p.l0.nclusters;
+        const uint32_t l1np = ix->nprobe == 0 ? n1 : ix->nprobe;
+        if (l1np < n1 / 2) top /= 2;
+    }
+    p.nprobe = np_flat;
+    p.top_nprobe = top;
+    p.n_order = n_order;
+    const uint32_t d = ix->d;
+    // the heap region also holds the sorted probe list (flat: nprobe, tree L0: top entries)
+    const uint32_t heap_cap = next_pow2(std::max({k, np_flat, top, 1u}));
+    uint32_t work = std::max({p.l1.max_n, heap_cap, 32u});
+    if (!ix->tree || any_filter) work = std::max(work, n1);
+    if (ix->tree) work = std::max({work, p.l0.max_n, p.l0.nclusters});
+    const uint32_t work_cap = next_pow2(work);
+    const uint32_t order_cap = std::max({np_flat, top, n_order, 1u});
+    uint32_t off = 0;
+    p.smem_qf = off;
+    off += (uint32_t)align_up((uint64_t)d * 4, 16);
+    p.smem_qw = off;
+    if (ix->u8) off += (uint32_t)align_up((uint64_t)(p.l1.qw_hoff + p.l1.n_hblocks * 16) * 4, 16);
+    p.smem_work = off;
+    off += work_cap * 8;
+    p.smem_heap = off;
+    off += heap_cap * 8;
+    p.smem_order = off;
+    off += (uint32_t)align_up((uint64_t)order_cap * 4, 16);
+    p.smem_total = off;
+    p.work_cap = work_cap;
+    p.heap_cap = heap_cap;
+    p.order_cap = order_cap;
+    if ((size_t)off + 2048 > ix->max_smem)
+        return fail(PDXG_ERR_CAPACITY, "per-query shared memory (" + std::to_string(off) +
+                                           " B) exceeds the device limit; cluster, k or nprobe too large");
+    L.u8 = ix->u8;
+    int threads = (int)ix->threads;
+    if (threads == 0) threads = 256;
+    L.threads = threads;
+    const int occ = search_occupancy(L.u8, threads, off);
+    if (occ <= 0) return fail(PDXG_ERR_CAPACITY, "search kernel cannot be resident with this configuration");
+    L.grid = (int)std::min<uint64_t>(nq, (uint64_t)occ * ix->num_sms);
+    return PDXG_OK;
+}
+
+int ensure_ws(pdxg_index* ix, uint32_t nq, uint32_t k) {
+    Workspace& w = ix->ws;
+    uint64_t cap;
+    if (nq > w.q_cap || !w.d_rq) {
+        cap = 0;
+        int rc = dev_grow(w.d_rq, cap, (uint64_t)nq * ix->d);
+        if (rc) return rc;
+        cap = 0;
+        if ((rc = dev_grow(w.d_norms, cap, nq))) return rc;
+        cap = 0;
+        if ((rc = dev_grow(w.d_counts, cap, nq))) return rc;
+        cap = 0;
+        if ((rc = dev_grow(w.d_q, cap, (uint64_t)nq * ix->d))) return rc;
+        w.q_cap = nq;
+        w.k_cap = 0;
+    }
+    if ((uint64_t)nq * k > (uint64_t)w.q_cap * w.k_cap || !w.d_ids) {
+        cap = 0;
+        int rc = dev_grow(w.d_ids, cap, (uint64_t)w.q_cap * k);
+        if (rc) return rc;
+        cap = 0;
+        if ((rc = dev_grow(w.d_dists, cap, (uint64_t)w.q_cap * k))) return rc;
+        w.k_cap = k;
+    }
+    if (!w.d_queue) PDXG_CUDA(cudaMalloc(&w.d_queue, sizeof(uint32_t)));
+    return PDXG_OK;
+}
+
+// Core device-side search: queries/ids/dists/counts are device pointers.
+int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, uint32_t flags,
+                       const uint32_t* d_order, uint32_t n_order, const uint32_t* d_sel,
+                       const uint32_t* d_pass, const int32_t* d_filter_of, bool any_filter,
+                       uint32_t* ids, float* dists, uint32_t* counts, cudaStream_t st) {
+    if (nq == 0) return PDXG_OK;
+    if (k == 0) {
+        PDXG_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, st));
+        return PDXG_OK;
+    }
+    int rc = ensure_ws(ix, nq, k);
+    if (rc) return rc;
+    const float* qp = q;
+    if (!(flags & PDXG_QUERY_TRANSFORMED)) {
+        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, ix->ws.d_norms,
+                                         ix->ws.d_rq, st));
+        qp = ix->ws.d_rq;
+    }
+    Launch L;
+    rc = plan_search(ix, nq, k, n_order, any_filter, L);
+    if (rc) return rc;
+    L.p.queries = qp;
+    L.p.order = d_order;
+    L.p.sel_bits = d_sel;
+    L.p.passing = d_pass;
+    L.p.filter_of = d_filter_of;
+    L.p.out_ids = ids;
+    L.p.out_dists = dists;
+    L.p.out_counts = counts;
+    L.p.queue = ix->ws.d_queue;
+    PDXG_CUDA(cudaMemsetAsync(ix->ws.d_queue, 0, sizeof(uint32_t), st));
+    PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
+    return PDXG_OK;
+}
+
+int check_index(const pdxg_index* ix) {
+    if (!ix) return fail(PDXG_ERR_INVALID_ARGUMENT, "index is NULL");
+    return PDXG_OK;
+}
+
+// Host-buffer search shared by pdxg_search / _with_order / filtered variants.
+int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
+                     const uint32_t* order, uint32_t n_order,
+                     const std::vector<uint32_t>* sel, const std::vector<uint32_t>* pass,
+                     const std::vector<int32_t>* filter_of, uint32_t* ids, float* dists,
+                     uint32_t* counts) {
+    if (!queries || !ids || !dists || !counts)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    int rc = ensure_ws(ix, nq, k);
+    if (rc) return rc;
+    Workspace& w = ix->ws;
+    cudaStream_t st = ix->stream;
+    PDXG_CUDA(cudaMemcpyAsync(w.d_q, queries, sizeof(float) * nq * ix->d, cudaMemcpyHostToDevice, st));
+    const uint32_t* d_order = nullptr;
+    if (order && n_order) {
+        uint64_t cap = w.order_cap;
+        if ((rc = dev_grow(w.d_order, cap, n_order))) return rc;
+        w.order_cap = (uint32_t)cap;
+        PDXG_CUDA(cudaMemcpyAsync(w.d_order, order, sizeof(uint32_t) * n_order, cudaMemcpyHostToDevice, st));
+        d_order = w.d_order;
+    }
+    const uint32_t* d_sel = nullptr;
+    const uint32_t* d_pass = nullptr;
+    const int32_t* d_fo = nullptr;
+    bool any_filter = false;
+    if (sel && !sel->empty()) {
+        any_filter = true;
+        if ((rc = dev_grow(w.d_sel, w.sel_cap, sel->size()))) return rc;
+        if ((rc = dev_grow(w.d_pass, w.pass_cap, pass->size()))) return rc;
+        uint64_t cap = w.fo_cap;
+        if ((rc = dev_grow(w.d_filter_of, cap, filter_of->size()))) return rc;
+        w.fo_cap = (uint32_t)cap;
+        PDXG_CUDA(cudaMemcpyAsync(w.d_sel, sel->data(), sel->size() * 4, cudaMemcpyHostToDevice, st));
+        PDXG_CUDA(cudaMemcpyAsync(w.d_pass, pass->data(), pass->size() * 4, cudaMemcpyHostToDevice, st));
+        PDXG_CUDA(cudaMemcpyAsync(w.d_filter_of, filter_of->data(), filter_of->size() * 4,
+                                  cudaMemcpyHostToDevice, st));
+        d_sel = w.d_sel;
+        d_pass = w.d_pass;
+        d_fo = w.d_filter_of;
+    }
+    rc = search_device_impl(ix, w.d_q, nq, k, flags, d_order, n_order, d_sel, d_pass, d_fo,
+                            any_filter, w.d_ids, w.d_dists, w.d_counts, st);
+    if (rc) return rc;
+    PDXG_CUDA(cudaMemcpyAsync(ids, w.d_ids, sizeof(uint32_t) * nq * k, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaMemcpyAsync(dists, w.d_dists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaMemcpyAsync(counts, w.d_counts, sizeof(uint32_t) * nq, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+// Selection bitmap + passing counts of one row-id list (CreatePredicateEvaluator,
+// index.hpp:436-446), in the device bitmap layout (one bit per cluster slot).
+void build_filter(const pdxg_index* ix, const uint64_t* rows, uint64_t n, uint32_t* sel,
+                  uint32_t* pass) {
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t r = rows[i];
+        if (r >= ix->rid_cluster.size()) continue;
+        const uint32_t c = ix->rid_cluster[r];
+        if (c == 0xFFFFFFFFu) continue;
+        const uint32_t pos = ix->rid_pos[r];
+        const uint32_t word = ix->l1.meta[c].sel_word + (pos >> 5);
+        const uint32_t bit = 1u << (pos & 31);
+        if (!(sel[word] & bit)) {
+            sel[word] |= bit;
+            pass[c]++;
+        }
+    }
+}
+
+}  // namespace
+
+// =============================================================================== C ABI
+extern "C" {
+
+const char* pdxg_last_error(void) { return g_err.c_str(); }
+
+int pdxg_load_buffer(const void* data, uint64_t size, int device, pdxg_index** out) {
+    if (!data) return fail(PDXG_ERR_INVALID_ARGUMENT, "data is NULL");
+    try {
+        return load_from_bytes(static_cast<const uint8_t*>(data), size, device, out);
+    } catch (const std::exception& e) {
+        return fail(PDXG_ERR_IO, e.what());
+    }
+}
+
+int pdxg_load(const char* path, int device, pdxg_index** out) {
+    if (!path) return fail(PDXG_ERR_INVALID_ARGUMENT, "path is NULL");
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) return fail(PDXG_ERR_IO, std::string("Failed to open file: ") + path);
+    const std::streamsize size = f.tellg();
+    f.seekg(0);
+    std::vector<uint8_t> buf((size_t)std::max<std::streamsize>(size, 0));
+    if (size > 0 && !f.read(reinterpret_cast<char*>(buf.data()), size))
+        return fail(PDXG_ERR_IO, std::string("Failed to read file: ") + path);
+    return pdxg_load_buffer(buf.data(), buf.size(), device, out);
+}
+
+void pdxg_free(pdxg_index* index) { free_index(index); }
+
+int pdxg_set_nprobe(pdxg_index* ix, uint32_t nprobe) {
+    if (int rc = check_index(ix)) return rc;
+    ix->nprobe = nprobe;
+    return PDXG_OK;
+}
+
+int pdxg_set_pruning_aggressiveness(pdxg_index* ix, float eps0) {
+    if (int rc = check_index(ix)) return rc;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    ix->eps0 = eps0;
+    return upload_ratios(ix);
+}
+
+int pdxg_set_threads_per_query(pdxg_index* ix, uint32_t threads) {
+    if (int rc = check_index(ix)) return rc;
+    if (threads != 0 && threads != 128 && threads != 256 && threads != 512)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "threads per query must be 0, 128, 256 or 512");
+    ix->threads = threads;
+    return PDXG_OK;
+}
+
+int pdxg_search(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
+                uint32_t* ids, float* distances, uint32_t* counts) {
+    if (int rc = check_index(ix)) return rc;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    return search_host_impl(ix, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr, ids,
+                            distances, counts);
+}
+
+int pdxg_search_device(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k,
+                       uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts,
+                       void* stream) {
+    if (int rc = check_index(ix)) return rc;
+    if (!queries || !ids || !distances || !counts)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ix->stream;
+    return search_device_impl(ix, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr,
+                              false, ids, distances, counts, st);
+}
+
+int pdxg_search_with_order(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k,
+                           const uint32_t* order, uint32_t n_order, uint32_t flags, uint32_t* ids,
+                           float* distances, uint32_t* counts) {
+    if (int rc = check_index(ix)) return rc;
+    if (!order && n_order) return fail(PDXG_ERR_INVALID_ARGUMENT, "order is NULL");
+    const uint32_t n1 = (uint32_t)ix->l1.fc.size();
+    for (uint32_t i = 0; i < n_order; ++i)
+        if (order[i] >= n1) return fail(PDXG_ERR_INVALID_ARGUMENT, "cluster id out of range in order");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    const uint32_t saved = ix->nprobe;
+    if (ix->tree && ix->nprobe == 0) ix->nprobe = n1;
+    int rc = search_host_impl(ix, queries, nq, k, flags, order, n_order ? n_order : 0, nullptr,
+                              nullptr, nullptr, ids, distances, counts);
+    ix->nprobe = saved;
+    return rc;
+}
+
+int pdxg_filtered_search_batch(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k,
+                               const uint64_t* row_ids, const uint64_t* offsets, uint32_t flags,
+                               uint32_t* ids, float* distances, uint32_t* counts) {
+    if (int rc = check_index(ix)) return rc;
+    if (!offsets) return fail(PDXG_ERR_INVALID_ARGUMENT, "offsets is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    const uint32_t words = ix->l1.sel_words;
+    const uint32_t ncl = (uint32_t)ix->l1.fc.size();
+    std::vector<int32_t> filter_of(nq, -1);
+    uint32_t nf = 0;
+    for (uint32_t q = 0; q < nq; ++q)
+        if (offsets[q] != UINT64_MAX) filter_of[q] = (int32_t)nf++;
+    std::vector<uint32_t> sel((uint64_t)nf * words, 0), pass((uint64_t)nf * ncl, 0);
+    for (uint32_t q = 0; q < nq; ++q) {
+        if (filter_of[q] < 0) continue;
+        uint64_t a = offsets[q], b = offsets[q + 1];
+        if (b == UINT64_MAX) {
+            // next query unfiltered: find the next valid end offset
+            uint32_t j = q + 1;
+            while (j < nq && offsets[j] == UINT64_MAX) ++j;
+            b = offsets[j];
+        }
+        if (b < a) return fail(PDXG_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+        if (!row_ids && b > a) return fail(PDXG_ERR_INVALID_ARGUMENT, "row_ids is NULL");
+        const uint32_t f = (uint32_t)filter_of[q];
+        build_filter(ix, row_ids + a, b - a, sel.data() + (uint64_t)f * words,
+                     pass.data() + (uint64_t)f * ncl);
+    }
+    if (nf == 0)
+        return search_host_impl(ix, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr,
+                                ids, distances, counts);
+    return search_host_impl(ix, queries, nq, k, flags, nullptr, 0, &sel, &pass, &filter_of, ids,
+                            distances, counts);
+}
+
+int pdxg_filtered_search(pdxg_index* ix, const float* query, uint32_t k, const uint64_t* row_ids,
+                         uint64_t n_row_ids, uint32_t flags, uint32_t* ids, float* distances,
+                         uint32_t* count) {
+    const uint64_t offsets[2] = {0, n_row_ids};
+    return pdxg_filtered_search_batch(ix, query, 1, k, row_ids, offsets, flags, ids, distances,
+                                      count);
+}
+
+int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, float* out) {
+    if (int rc = check_index(ix)) return rc;
+    if (!queries || !out) return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    int rc = ensure_ws(ix, nq, 1);
+    if (rc) return rc;
+    cudaStream_t st = ix->stream;
+    PDXG_CUDA(cudaMemcpyAsync(ix->ws.d_q, queries, sizeof(float) * nq * ix->d, cudaMemcpyHostToDevice, st));
+    PDXG_CUDA(launch_prepare_queries(ix->ws.d_q, nq, ix->d, ix->d_rot, ix->normalized,
+                                     ix->ws.d_norms, ix->ws.d_rq, st));
+    PDXG_CUDA(cudaMemcpyAsync(out, ix->ws.d_rq, sizeof(float) * nq * ix->d, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+int pdxg_index_type(const pdxg_index* ix) { return ix ? ix->type : -1; }
+uint32_t pdxg_num_dimensions(const pdxg_index* ix) { return ix ? ix->d : 0; }
+uint32_t pdxg_num_clusters(const pdxg_index* ix) { return ix ? (uint32_t)ix->l1.fc.size() : 0; }
+uint32_t pdxg_nprobe(const pdxg_index* ix) { return ix ? ix->nprobe : 0; }
+uint64_t pdxg_num_embeddings(const pdxg_index* ix) { return ix ? ix->l1.total_vectors : 0; }
+
+uint32_t pdxg_cluster_size(const pdxg_index* ix, uint32_t cluster_id) {
+    if (!ix || cluster_id >= ix->l1.n.size()) return 0;
+    return ix->l1.n[cluster_id];
+}
+
+int pdxg_cluster_row_ids(const pdxg_index* ix, uint32_t cluster_id, uint32_t* out,
+                         uint32_t capacity) {
+    if (int rc = check_index(ix)) return rc;
+    if (cluster_id >= ix->l1.n.size()) return fail(PDXG_ERR_INVALID_ARGUMENT, "cluster_id out of range");
+    const uint32_t n = ix->l1.n[cluster_id];
+    if (capacity < n || (!out && n)) return fail(PDXG_ERR_INVALID_ARGUMENT, "output buffer too small");
+    std::memcpy(out, ix->l1.ids.data() + ix->l1.ids_start[cluster_id], (size_t)n * 4);
+    return PDXG_OK;
+}
+
+uint64_t pdxg_in_memory_size_in_bytes(const pdxg_index* ix) {
+    if (!ix) return 0;
+    uint64_t s = ix->arena_bytes;
+    s += (ix->l1.meta.size() + ix->l0.meta.size()) * sizeof(DevCluster);
+    s += (ix->l1.centroids.size() + ix->l0.centroids.size() + ix->rotation.size() + ix->d) * 4;
+    return s;
+}
+
+int pdxg_save(pdxg_index* ix, const char* path) {
+    if (int rc = check_index(ix)) return rc;
+    if (!path) return fail(PDXG_ERR_INVALID_ARGUMENT, "path is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    std::vector<uint8_t> img(ix->arena_bytes);
+    PDXG_CUDA(cudaMemcpy(img.data(), ix->arena, ix->arena_bytes, cudaMemcpyDeviceToHost));
+    std::ofstream out(path, std::ios::binary);
+    if (!out) return fail(PDXG_ERR_IO, std::string("Failed to open file for writing: ") + path);
+    auto w32 = [&](uint32_t v) { out.write(reinterpret_cast<const char*>(&v), 4); };
+    const uint8_t type = (uint8_t)ix->type;
+    out.write(reinterpret_cast<const char*>(&type), 1);
+    w32(ix->rot_rows);
+    w32(ix->rot_cols);
+    out.write(reinterpret_cast<const char*>(ix->rotation.data()), ix->rotation.size() * 4);
+    auto write_level = [&](const HostLevel& lv) {
+        for (size_t i = 0; i < lv.meta.size(); ++i) {
+            w32(lv.n[i]);
+            w32(lv.max_cap[i]);
+        }
+        std::vector<uint8_t> tmp;
+        for (size_t i = 0; i < lv.meta.size(); ++i) {
+            const DevCluster& m = lv.meta[i];
+            const uint64_t n = m.n, np = m.n_pad;
+            if (!lv.u8) {
+                for (uint32_t j = 0; j < lv.dv; ++j)
+                    out.write(reinterpret_cast<const char*>(img.data() + m.vert_off + (uint64_t)j * np * 4), n * 4);
+                for (uint32_t b = 0; b < lv.n_hblocks; ++b)
+                    out.write(reinterpret_cast<const char*>(img.data() + m.hor_off + (uint64_t)b * np * kHDim * 4),
+                              n * kHDim * 4);
+            } else {
+                const uint32_t full = lv.dv / 4, rem = lv.dv % 4;
+                for (uint32_t g = 0; g < full; ++g)
+                    out.write(reinterpret_cast<const char*>(img.data() + m.vert_off + (uint64_t)g * np * 4), n * 4);
+                if (rem) {
+                    tmp.assign(n * rem, 0);
+                    const uint8_t* src = img.data() + m.vert_off + (uint64_t)full * np * 4;
+                    for (uint64_t v = 0; v < n; ++v)
+                        for (uint32_t t = 0; t < rem; ++t) tmp[v * rem + t] = src[v * 4 + t];
+                    out.write(reinterpret_cast<const char*>(tmp.data()), tmp.size());
+                }
+                for (uint32_t b = 0; b < lv.n_hblocks; ++b)
+                    out.write(reinterpret_cast<const char*>(img.data() + m.hor_off + (uint64_t)b * np * kHDim),
+                              n * kHDim);
+            }
+        }
+        for (size_t i = 0; i < lv.meta.size(); ++i)
+            out.write(reinterpret_cast<const char*>(lv.ids.data() + lv.ids_start[i]), (size_t)lv.n[i] * 4);
+    };
+    w32(ix->d);
+    w32(ix->dv);
+    w32(ix->dh);
+    w32((uint32_t)ix->l1.meta.size());
+    if (ix->tree) {
+        w32((uint32_t)ix->l0.meta.size());
+        write_level(ix->l0);
+    }
+    write_level(ix->l1);
+    const uint8_t norm = ix->normalized ? 1 : 0;
+    out.write(reinterpret_cast<const char*>(&norm), 1);
+    const std::vector<float>& cent = ix->tree ? ix->l0.centroids : ix->l1.centroids;
+    out.write(reinterpret_cast<const char*>(cent.data()), cent.size() * 4);
+    if (ix->u8) {
+        out.write(reinterpret_cast<const char*>(&ix->base), 4);
+        out.write(reinterpret_cast<const char*>(&ix->scale), 4);
+    }
+    if (!out) return fail(PDXG_ERR_IO, std::string("Failed to write file: ") + path);
+    return PDXG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,838 @@
+// PDXearch on B200: one CTA per query, persistent over a batch of queries.
+//
+// Each CTA walks one query's clusters in probe order with the reference's sequential
+// semantics, so results are identical to PDXearch::Search / FilteredSearch
+// (searcher.hpp:596-856) on the same prepared query:
+//   * probe order: exact F32 centroid distances in the reference's AVX2 reduction order,
+//     block radix-select of the nprobe nearest, bitonic sort (searcher.hpp:181-215);
+//   * Start for clusters met while the heap holds fewer than k entries: full distances,
+//     only the best k - |heap| are pushed (searcher.hpp:217-281);
+//   * Warmup: vertical dims in the DIMENSIONS_FETCHING_SIZES steps until >= ceil(0.8 n)
+//     vectors fail the ADSampling bound (searcher.hpp:374-435);
+//   * Prune: survivors compacted with __ballot_sync/__popc, gathered 64-dim horizontal
+//     blocks, then the remaining vertical dims in 64-dim steps, re-pruning after each block
+//     (searcher.hpp:437-540);
+//   * MergeIntoHeap with strict-< admission in survivor order (searcher.hpp:542-566).
+// Distances: U8 uses __vabsdiffu4 + __dp4a into exact uint32 (the exact scalar semantics of
+// scalar_computers.hpp:137-194); F32 vertical is one fused multiply-add per dimension and F32
+// horizontal reproduces avx2_computers.hpp:47-98 (8 FMA lanes, pairwise double reduction).
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pdxg_common.cuh"
+
+namespace pdxg {
+
+__constant__ uint32_t c_fetch_sizes[kNumFetchSizes] = {16,  16,  32,  32,  32,   32,   64,
+                                                       64,  64,  64,  128, 128,  128,  128,
+                                                       256, 256, 512, 1024, 2048, 16384};
+
+constexpr uint32_t kMaskU8 = 0x7FFFFFFFu;                 // numeric_limits<u32>::max() / 2
+#define PDXG_MASK_F32 (FLT_MAX / 2.0f)                     // numeric_limits<float>::max() / 2
+
+// ------------------------------------------------------------------------------------------
+// Per-CTA state in shared memory.
+struct Shared {
+    float* qf;          // prepared query, f32 [d]
+    uint32_t* qw;       // U8 query words: [n_vwords] vertical groups, then [n_hblocks*16]
+    uint32_t* dist;     // [work_cap] partial distances (u32, or f32 bits)
+    uint32_t* pos;      // [work_cap] survivor positions
+    float* hd;          // [heap_cap] heap distances
+    uint32_t* hid;      // [heap_cap] heap row ids
+    uint32_t* order;    // [order_cap] cluster visit order
+    uint64_t* sortw;    // work region viewed as u64 [work_cap]
+    uint64_t* sorth;    // heap region viewed as u64 [heap_cap]
+};
+
+struct Scalars {
+    uint32_t warp[32];
+    uint32_t hist[256];
+    uint32_t sc[4];
+    uint32_t hsize;
+    uint32_t top_slot;
+    float top;
+    uint32_t query;
+    uint32_t n_order;
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
+
+template <int T>
+__device__ __forceinline__ uint32_t block_sum(uint32_t x, Scalars& s) {
+    constexpr int NW = T / 32;
+    x = __reduce_add_sync(0xffffffffu, x);
+    if (lane_id() == 0) s.warp[warp_id()] = x;
+    __syncthreads();
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) tot += s.warp[w];
+    __syncthreads();
+    return tot;
+}
+
+// Order-preserving compaction of i in [0, n) with pred(i): out[rank] = val(i).
+// In-place use (out aliasing the array val() reads) is safe: every element of a chunk is
+// read before the chunk's writes, and writes never reach past the current chunk.
+template <int T, class Pred, class Val>
+__device__ uint32_t block_compact(uint32_t n, Pred pred, Val val, uint32_t* out, Scalars& s) {
+    constexpr int NW = T / 32;
+    const uint32_t lane = lane_id(), warp = warp_id();
+    uint32_t total = 0;
+    for (uint32_t c0 = 0; c0 < n; c0 += T) {
+        const uint32_t i = c0 + threadIdx.x;
+        const bool in = i < n;
+        const uint32_t v = in ? val(i) : 0u;
+        const bool p = in && pred(i, v);
+        const unsigned b = __ballot_sync(0xffffffffu, p);
+        if (lane == 0) s.warp[warp] = __popc(b);
+        __syncthreads();
+        uint32_t off = total, ctot = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const uint32_t c = s.warp[w];
+            off += (w < (int)warp) ? c : 0u;
+            ctot += c;
+        }
+        if (p) out[off + __popc(b & ((1u << lane) - 1u))] = v;
+        total += ctot;
+        __syncthreads();
+    }
+    return total;
+}
+
+// Exact selection: kth = the m-th smallest key (1 <= m <= n), less = #keys < kth.
+template <int T>
+__device__ void block_radix_select(const uint32_t* keys, uint32_t n, uint32_t m, Scalars& s,
+                                   uint32_t& kth, uint32_t& less) {
+    uint32_t prefix = 0, mask = 0, rem = m, acc_less = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += T) s.hist[i] = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += T) {
+            const uint32_t k = keys[i];
+            if ((k & mask) == prefix) atomicAdd(&s.hist[(k >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const uint32_t lane = lane_id();
+            uint32_t loc[8], sum = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                loc[j] = s.hist[lane * 8 + j];
+                sum += loc[j];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= (uint32_t)off) incl += t;
+            }
+            const uint32_t excl = incl - sum;
+            const bool mine = excl < rem && rem <= incl;
+            const unsigned bm = __ballot_sync(0xffffffffu, mine);
+            if (lane == (uint32_t)(__ffs(bm) - 1)) {
+                uint32_t c = excl;
+                int b = 0;
+                for (; b < 7; ++b) {
+                    if (c + loc[b] >= rem) break;
+                    c += loc[b];
+                }
+                s.sc[0] = lane * 8 + b;
+                s.sc[1] = c;
+            }
+        }
+        __syncthreads();
+        const uint32_t bin = s.sc[0], cum = s.sc[1];
+        prefix |= bin << shift;
+        mask |= 0xFFu << shift;
+        rem -= cum;
+        acc_less += cum;
+        __syncthreads();
+    }
+    kth = prefix;
+    less = acc_less;
+}
+
+// Ascending bitonic sort of N (power of two) u64 keys in shared memory.
+template <int T>
+__device__ void block_bitonic_sort(uint64_t* a, uint32_t N) {
+    for (uint32_t size = 2; size <= N; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < (N >> 1); i += T) {
+                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
+                const uint32_t hi = lo + stride;
+                const bool asc = (lo & size) == 0;
+                const uint64_t x = a[lo], y = a[hi];
+                if ((x > y) == asc) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t next_pow2(uint32_t x) {
+    return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
+}
+
+// ------------------------------------------------------------------------------------------
+// Distances.
+
+// avx2_computers.hpp:47-98 over one 64-dim row, 8 threads per row (sub = lane & 7): lane j
+// accumulates dims j, j+8, ..., j+56 with FMA; lanes 0 of each 8-group return the f32 result.
+__device__ __forceinline__ float horiz64_f32_group8(const float* q, const float* x, uint32_t sub,
+                                                    bool active) {
+    float acc = 0.0f;
+    if (active) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const float d = __fsub_rn(q[sub + 8 * t], __ldg(x + sub + 8 * t));
+            acc = __fmaf_rn(d, d, acc);
+        }
+    }
+    double s = (double)acc + (double)__shfl_down_sync(0xffffffffu, acc, 4, 8);
+    s = s + __shfl_down_sync(0xffffffffu, s, 2, 8);
+    s = s + __shfl_down_sync(0xffffffffu, s, 1, 8);
+    return (float)s;
+}
+
+// Full-length avx2 Horizontal(q, x, d) for centroid probing, 8 threads per vector.
+__device__ __forceinline__ float horiz_f32_group8(const float* q, const float* x, uint32_t d,
+                                                  uint32_t sub, bool active) {
+    float acc = 0.0f;
+    const uint32_t full = d & ~7u;
+    if (active) {
+        for (uint32_t i = 0; i < full; i += 8) {
+            const float t = __fsub_rn(q[i + sub], __ldg(x + i + sub));
+            acc = __fmaf_rn(t, t, acc);
+        }
+    }
+    double s = (double)acc + (double)__shfl_down_sync(0xffffffffu, acc, 4, 8);
+    s = s + __shfl_down_sync(0xffffffffu, s, 2, 8);
+    s = s + __shfl_down_sync(0xffffffffu, s, 1, 8);
+    if (active && sub == 0) {
+        for (uint32_t i = full; i < d; ++i) {
+            const float t = __fsub_rn(q[i], __ldg(x + i));
+            s += (double)__fmul_rn(t, t);
+        }
+    }
+    return (float)s;
+}
+
+__device__ __forceinline__ uint32_t sqdiff4(uint32_t a, uint32_t b, uint32_t acc) {
+    const uint32_t d = __vabsdiffu4(a, b);
+    return __dp4a(d, d, acc);
+}
+
+// ------------------------------------------------------------------------------------------
+// Per-level search state and operations (T threads, one query).
+template <int T, bool U8>
+struct LevelOps {
+    static constexpr bool u8 = U8;
+    const SearchParams& p;
+    const DevLevel& lv;
+    Shared& sh;
+    Scalars& s;
+    int filter;  // -1 = unfiltered
+
+    __device__ LevelOps(const SearchParams& p_, const DevLevel& lv_, Shared& sh_, Scalars& s_,
+                        int filter_)
+        : p(p_), lv(lv_), sh(sh_), s(s_), filter(filter_) {}
+
+    __device__ __forceinline__ const uint32_t* vert(const DevCluster& c) const {
+        return reinterpret_cast<const uint32_t*>(p.arena + c.vert_off);
+    }
+    __device__ __forceinline__ const uint32_t* ids(const DevCluster& c) const {
+        return reinterpret_cast<const uint32_t*>(p.arena + c.ids_off);
+    }
+    __device__ __forceinline__ float reported(uint32_t raw) const {
+        return u8 ? __fmul_rn(__uint2float_rn(raw), lv.inv_scale_sq) : __uint_as_float(raw);
+    }
+    __device__ __forceinline__ float thr_f(uint32_t cur) const {
+        const float r = (cur == lv.d) ? 1.0f : __ldg(p.ratios + cur);
+        return __fmul_rn(s.top, r);
+    }
+    // Pruning threshold in the raw distance domain, as u32 bits (searcher.hpp:75-91).
+    __device__ __forceinline__ uint32_t thr_raw(uint32_t cur) const {
+        const float f = thr_f(cur);
+        if (!u8) return __float_as_uint(f);
+        const float scaled = __fmul_rn(f, lv.scale_sq);
+        return scaled >= 4294967296.0f ? 0xFFFFFFFFu : __float2uint_rz(scaled);
+    }
+    // dist < threshold, in the level's distance domain (F32 compares as floats).
+    __device__ __forceinline__ bool below(uint32_t raw, uint32_t thr) const {
+        return u8 ? raw < thr : __uint_as_float(raw) < __uint_as_float(thr);
+    }
+    __device__ __forceinline__ bool selected(const DevCluster& c, uint32_t v) const {
+        if (filter < 0) return true;
+        const uint32_t* bits = p.sel_bits + (size_t)filter * lv.sel_words + c.sel_word;
+        return (__ldg(bits + (v >> 5)) >> (v & 31)) & 1u;
+    }
+    __device__ __forceinline__ uint32_t mask_raw() const {
+        return u8 ? kMaskU8 : __float_as_uint(PDXG_MASK_F32);
+    }
+
+    // Vertical dims [d0, d1) for all vectors; returns #vectors with dist >= thr (counted only
+    // when count is set). For U8, d0 is a multiple of 4; a trailing partial group is reached
+    // only with d1 == dv and its padding bytes are zero in both query and data.
+    __device__ uint32_t vertical_all(const DevCluster& c, uint32_t d0, uint32_t d1, bool count,
+                                     uint32_t thr) {
+        const uint32_t* base = vert(c);
+        const uint32_t n = c.n, np = c.n_pad;
+        uint32_t pruned = 0;
+        if constexpr (U8) {
+            const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
+            for (uint32_t v = threadIdx.x; v < n; v += T) {
+                uint32_t acc = sh.dist[v];
+                uint32_t g = g0;
+                for (; g + 4 <= g1; g += 4) {
+                    const uint32_t x0 = __ldg(base + (size_t)g * np + v);
+                    const uint32_t x1 = __ldg(base + (size_t)(g + 1) * np + v);
+                    const uint32_t x2 = __ldg(base + (size_t)(g + 2) * np + v);
+                    const uint32_t x3 = __ldg(base + (size_t)(g + 3) * np + v);
+                    acc = sqdiff4(sh.qw[g], x0, acc);
+                    acc = sqdiff4(sh.qw[g + 1], x1, acc);
+                    acc = sqdiff4(sh.qw[g + 2], x2, acc);
+                    acc = sqdiff4(sh.qw[g + 3], x3, acc);
+                }
+                for (; g < g1; ++g) acc = sqdiff4(sh.qw[g], __ldg(base + (size_t)g * np + v), acc);
+                sh.dist[v] = acc;
+                pruned += (count && acc >= thr) ? 1u : 0u;
+            }
+        } else {
+            const float* fb = reinterpret_cast<const float*>(base);
+            for (uint32_t v = threadIdx.x; v < n; v += T) {
+                float acc = __uint_as_float(sh.dist[v]);
+                uint32_t j = d0;
+                for (; j + 4 <= d1; j += 4) {
+                    const float x0 = __ldg(fb + (size_t)j * np + v);
+                    const float x1 = __ldg(fb + (size_t)(j + 1) * np + v);
+                    const float x2 = __ldg(fb + (size_t)(j + 2) * np + v);
+                    const float x3 = __ldg(fb + (size_t)(j + 3) * np + v);
+                    float t = __fsub_rn(sh.qf[j], x0);
+                    acc = __fmaf_rn(t, t, acc);
+                    t = __fsub_rn(sh.qf[j + 1], x1);
+                    acc = __fmaf_rn(t, t, acc);
+                    t = __fsub_rn(sh.qf[j + 2], x2);
+                    acc = __fmaf_rn(t, t, acc);
+                    t = __fsub_rn(sh.qf[j + 3], x3);
+                    acc = __fmaf_rn(t, t, acc);
+                }
+                for (; j < d1; ++j) {
+                    const float t = __fsub_rn(sh.qf[j], __ldg(fb + (size_t)j * np + v));
+                    acc = __fmaf_rn(t, t, acc);
+                }
+                sh.dist[v] = __float_as_uint(acc);
+                pruned += (count && acc >= __uint_as_float(thr)) ? 1u : 0u;
+            }
+        }
+        return count ? block_sum<T>(pruned, s) : 0u;
+    }
+
+    // Vertical dims [d0, d1) for the first npos listed positions (gathered access).
+    __device__ void vertical_pos(const DevCluster& c, uint32_t d0, uint32_t d1, uint32_t npos) {
+        const uint32_t* base = vert(c);
+        const uint32_t np = c.n_pad;
+        if constexpr (U8) {
+            const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
+            for (uint32_t i = threadIdx.x; i < npos; i += T) {
+                const uint32_t v = sh.pos[i];
+                uint32_t acc = sh.dist[v];
+                for (uint32_t g = g0; g < g1; ++g)
+                    acc = sqdiff4(sh.qw[g], __ldg(base + (size_t)g * np + v), acc);
+                sh.dist[v] = acc;
+            }
+        } else {
+            const float* fb = reinterpret_cast<const float*>(base);
+            for (uint32_t i = threadIdx.x; i < npos; i += T) {
+                const uint32_t v = sh.pos[i];
+                float acc = __uint_as_float(sh.dist[v]);
+                for (uint32_t j = d0; j < d1; ++j) {
+                    const float t = __fsub_rn(sh.qf[j], __ldg(fb + (size_t)j * np + v));
+                    acc = __fmaf_rn(t, t, acc);
+                }
+                sh.dist[v] = __float_as_uint(acc);
+            }
+        }
+        __syncthreads();
+    }
+
+    // Adds horizontal block b to the distances of positions[0, npos) (all vectors when
+    // all_vectors is set, npos = n).
+    __device__ void horizontal(const DevCluster& c, uint32_t b, uint32_t npos, bool all_vectors) {
+        const uint32_t np = c.n_pad;
+        const uint32_t lane = lane_id();
+        if constexpr (U8) {
+            const uint8_t* hb = p.arena + c.hor_off + (size_t)b * np * kHDim;
+            const uint32_t* qh = sh.qw + lv.qw_hoff + b * 16;
+            const uint32_t sub = lane & 3;
+            const uint32_t per_pass = T / 4;
+            const uint4 q4 = *reinterpret_cast<const uint4*>(qh + sub * 4);
+            for (uint32_t base = 0; base < npos; base += per_pass) {
+                const uint32_t i = base + (threadIdx.x >> 2);
+                const bool active = i < npos;
+                const uint32_t v = active ? (all_vectors ? i : sh.pos[i]) : 0u;
+                uint32_t acc = 0;
+                if (active) {
+                    const uint4 x = __ldg(reinterpret_cast<const uint4*>(hb + (size_t)v * kHDim) + sub);
+                    acc = sqdiff4(q4.x, x.x, acc);
+                    acc = sqdiff4(q4.y, x.y, acc);
+                    acc = sqdiff4(q4.z, x.z, acc);
+                    acc = sqdiff4(q4.w, x.w, acc);
+                }
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                if (active && sub == 0) sh.dist[v] += acc;
+            }
+        } else {
+            const float* hb = reinterpret_cast<const float*>(p.arena + c.hor_off) + (size_t)b * np * kHDim;
+            const float* qh = sh.qf + lv.dv + b * kHDim;
+            const uint32_t sub = lane & 7;
+            const uint32_t per_pass = T / 8;
+            for (uint32_t base = 0; base < npos; base += per_pass) {
+                const uint32_t i = base + (threadIdx.x >> 3);
+                const bool active = i < npos;
+                const uint32_t v = active ? (all_vectors ? i : sh.pos[i]) : 0u;
+                const float h = horiz64_f32_group8(qh, hb + (size_t)v * kHDim, sub, active);
+                if (active && sub == 0)
+                    sh.dist[v] = __float_as_uint(__fadd_rn(__uint_as_float(sh.dist[v]), h));
+            }
+        }
+        __syncthreads();
+    }
+
+    __device__ void zero_dist(uint32_t n) {
+        for (uint32_t v = threadIdx.x; v < n; v += T) sh.dist[v] = 0u;
+        __syncthreads();
+    }
+
+    __device__ void recompute_top() {
+        if (threadIdx.x < 32) {
+            const uint32_t lane = lane_id();
+            float best = -1.0f;
+            uint32_t slot = 0xFFFFFFFFu;
+            for (uint32_t i = lane; i < s.hsize; i += 32) {
+                const float v = sh.hd[i];
+                if (v > best || (v == best && i < slot)) {
+                    best = v;
+                    slot = i;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                const uint32_t os = __shfl_xor_sync(0xffffffffu, slot, off);
+                if (ob > best || (ob == best && os < slot)) {
+                    best = ob;
+                    slot = os;
+                }
+            }
+            if (lane == 0) {
+                s.top = best;
+                s.top_slot = slot;
+            }
+        }
+        __syncthreads();
+    }
+
+    // Pushes the m smallest raw distances of the cluster (searcher.hpp:256-280).
+    __device__ void push_smallest(const DevCluster& c, uint32_t m) {
+        if (m == 0) return;
+        uint32_t kth, less;
+        block_radix_select<T>(sh.dist, c.n, m, s, kth, less);
+        const uint32_t* idp = ids(c);
+        uint32_t* dist = sh.dist;
+        const uint32_t nl = block_compact<T>(
+            c.n, [&](uint32_t, uint32_t v) { return dist[v] < kth; }, [](uint32_t i) { return i; },
+            sh.pos, s);
+        const uint32_t ties_needed = m - nl;
+        // ties at the m-th key: lowest positions first
+        const uint32_t nt = block_compact<T>(
+            c.n, [&](uint32_t, uint32_t v) { return dist[v] == kth; }, [](uint32_t i) { return i; },
+            sh.pos + nl, s);
+        (void)nt;
+        const uint32_t hs = s.hsize;
+        for (uint32_t j = threadIdx.x; j < m; j += T) {
+            const uint32_t v = sh.pos[j];
+            sh.hd[hs + j] = reported(dist[v]);
+            sh.hid[hs + j] = __ldg(idp + v);
+        }
+        (void)ties_needed;
+        __syncthreads();
+        if (threadIdx.x == 0) s.hsize = hs + m;
+        __syncthreads();
+        recompute_top();
+    }
+
+    // searcher.hpp:217-281
+    __device__ void start(const DevCluster& c, uint32_t k) {
+        zero_dist(c.n);
+        vertical_all(c, 0, lv.dv, false, 0);
+        __syncthreads();
+        for (uint32_t b = 0; b < lv.n_hblocks; ++b) horizontal(c, b, c.n, true);
+        uint32_t m = k - s.hsize;
+        if (m > c.n) m = c.n;
+        push_smallest(c, m);
+    }
+
+    // searcher.hpp:283-372
+    __device__ void filtered_start(const DevCluster& c, uint32_t k, uint32_t passing) {
+        zero_dist(c.n);
+        const uint32_t nsel = block_compact<T>(
+            c.n, [&](uint32_t i, uint32_t) { return selected(c, i); }, [](uint32_t i) { return i; },
+            sh.pos, s);
+        for (uint32_t b = 0; b < lv.n_hblocks; ++b) horizontal(c, b, nsel, false);
+        const float pct = __fdiv_rn((float)passing, (float)c.n);
+        if (pct > (1.0f - kSelectivity)) {
+            vertical_all(c, 0, lv.dv, false, 0);
+            __syncthreads();
+        } else {
+            vertical_pos(c, 0, lv.dv, nsel);
+        }
+        uint32_t m = k - s.hsize;
+        if (m > passing) m = passing;
+        const uint32_t mask = mask_raw();
+        for (uint32_t v = threadIdx.x; v < c.n; v += T)
+            if (!selected(c, v)) sh.dist[v] = mask;
+        __syncthreads();
+        push_smallest(c, m);
+    }
+
+    // Warmup + Prune + MergeIntoHeap for one cluster with a full heap.
+    __device__ void prune_cluster(const DevCluster& c, uint32_t k, uint32_t passing) {
+        const uint32_t n = c.n;
+        uint32_t cur = 0;
+        zero_dist(n);
+        bool skip_warmup = false;
+        if (filter >= 0) {
+            const uint32_t mask = mask_raw();
+            for (uint32_t v = threadIdx.x; v < n; v += T)
+                if (!selected(c, v)) sh.dist[v] = mask;
+            __syncthreads();
+            const float pct = __fdiv_rn((float)passing, (float)n);
+            skip_warmup = pct < (1.0f - kSelectivity);
+        }
+        if (!skip_warmup) {
+            const uint32_t needed = (uint32_t)ceilf(__fmul_rn(kSelectivity, (float)n));
+            uint32_t n_pruned = 0, step = 0;
+            while (n_pruned < needed && cur < lv.dv) {
+                uint32_t last = cur + c_fetch_sizes[step < kNumFetchSizes ? step : kNumFetchSizes - 1];
+                if (last > lv.dv) last = lv.dv;
+                const uint32_t thr = thr_raw(last);
+                n_pruned = vertical_all(c, cur, last, true, thr);
+                cur = last;
+                ++step;
+            }
+        }
+        // Prune (searcher.hpp:437-540)
+        uint32_t thr = thr_raw(cur);
+        uint32_t* dist = sh.dist;
+        const LevelOps* self = this;  // captured by the predicates
+        uint32_t nsurv = block_compact<T>(
+            n,
+            [&](uint32_t i, uint32_t) { return self->below(dist[i], thr) && self->selected(c, i); },
+            [](uint32_t i) { return i; }, sh.pos, s);
+        uint32_t cur_v = cur, cur_h = 0;
+        while (lv.dh && nsurv && cur_h < lv.dh) {
+            horizontal(c, cur_h / kHDim, nsurv, false);
+            cur_h += kHDim;
+            cur += kHDim;
+            thr = thr_raw(cur);
+            uint32_t* pos = sh.pos;
+            nsurv = block_compact<T>(
+                nsurv, [&](uint32_t, uint32_t v) { return self->below(dist[v], thr); },
+                [&](uint32_t i) { return pos[i]; }, sh.pos, s);
+        }
+        while (nsurv && cur_v < lv.dv) {
+            uint32_t last = cur_v + kHDim;
+            if (last > lv.dv) last = lv.dv;
+            vertical_pos(c, cur_v, last, nsurv);
+            cur = (cur + kHDim < lv.d) ? cur + kHDim : lv.d;
+            cur_v = last;
+            thr = thr_raw(cur);
+            uint32_t* pos = sh.pos;
+            nsurv = block_compact<T>(
+                nsurv, [&](uint32_t, uint32_t v) { return self->below(dist[v], thr); },
+                [&](uint32_t i) { return pos[i]; }, sh.pos, s);
+            if (cur == lv.d) break;
+        }
+        // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, survivor order.
+        if (nsurv) {
+            const uint32_t* idp = ids(c);
+            if (threadIdx.x < 32) {
+                const uint32_t lane = lane_id();
+                float top = s.top;
+                uint32_t slot = s.top_slot;
+                uint32_t hsize = s.hsize;
+                for (uint32_t i = 0; i < nsurv; ++i) {
+                    const uint32_t v = sh.pos[i];
+                    const float dd = reported(sh.dist[v]);
+                    if (hsize < k || dd < top) {
+                        if (lane == 0) {
+                            const uint32_t at = (hsize >= k) ? slot : hsize;
+                            sh.hd[at] = dd;
+                            sh.hid[at] = __ldg(idp + v);
+                        }
+                        if (hsize < k) ++hsize;
+                        __syncwarp();
+                        float best = -1.0f;
+                        uint32_t bs = 0xFFFFFFFFu;
+                        for (uint32_t j = lane; j < hsize; j += 32) {
+                            const float x = sh.hd[j];
+                            if (x > best || (x == best && j < bs)) {
+                                best = x;
+                                bs = j;
+                            }
+                        }
+#pragma unroll
+                        for (int off = 16; off > 0; off >>= 1) {
+                            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                            const uint32_t os = __shfl_xor_sync(0xffffffffu, bs, off);
+                            if (ob > best || (ob == best && os < bs)) {
+                                best = ob;
+                                bs = os;
+                            }
+                        }
+                        top = best;
+                        slot = bs;
+                    }
+                }
+                if (lane == 0) {
+                    s.top = top;
+                    s.top_slot = slot;
+                    s.hsize = hsize;
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // Visits clusters order[0, nvisit) (searcher.hpp:655-721 / 776-853).
+    __device__ void run(uint32_t k, uint32_t nvisit) {
+        if (threadIdx.x == 0) {
+            s.hsize = 0;
+            s.top = 0.0f;
+            s.top_slot = 0;
+        }
+        __syncthreads();
+        for (uint32_t ci = 0; ci < nvisit; ++ci) {
+            const uint32_t cidx = sh.order[ci];
+            const DevCluster c = lv.clusters[cidx];
+            uint32_t passing = 0;
+            if (filter >= 0) {
+                passing = __ldg(p.passing + (size_t)filter * lv.nclusters + cidx);
+                if (passing == 0) continue;
+            }
+            if (c.n == 0) continue;
+            if (s.hsize < k) {
+                if (filter >= 0)
+                    filtered_start(c, k, passing);
+                else
+                    start(c, k);
+                continue;
+            }
+            prune_cluster(c, k, passing);
+        }
+    }
+
+    // Sorts the heap ascending into sh.sortw; returns the result count (searcher.hpp:568-585).
+    __device__ uint32_t sort_heap(uint32_t k) {
+        uint32_t hs = s.hsize;
+        const uint32_t N = next_pow2(hs ? hs : 1);
+        for (uint32_t i = threadIdx.x; i < N; i += T)
+            sh.sortw[i] = (i < hs) ? ((uint64_t)__float_as_uint(sh.hd[i]) << 32) | sh.hid[i]
+                                   : ~0ull;
+        __syncthreads();
+        block_bitonic_sort<T>(sh.sortw, N);
+        // drop one FLT_MAX initialisation element when it is the maximum
+        if (hs && __uint_as_float((uint32_t)(sh.sortw[hs - 1] >> 32)) == FLT_MAX) --hs;
+        return hs < k ? hs : k;
+    }
+
+    // Probe order over the level's centroids: nearest `nprobe` sorted ascending into sh.order.
+    __device__ uint32_t probe(uint32_t nprobe) {
+        const uint32_t nc = lv.nclusters;
+        const uint32_t lane = lane_id(), sub = lane & 7;
+        for (uint32_t base = 0; base < nc; base += T / 8) {
+            const uint32_t cidx = base + (threadIdx.x >> 3);
+            const bool active = cidx < nc;
+            const float d = horiz_f32_group8(sh.qf, lv.centroids + (size_t)(active ? cidx : 0) * lv.d,
+                                             lv.d, sub, active);
+            if (active && sub == 0) sh.dist[cidx] = __float_as_uint(d);
+        }
+        __syncthreads();
+        const uint32_t m = nprobe < nc ? nprobe : nc;
+        uint32_t kth, less;
+        block_radix_select<T>(sh.dist, nc, m, s, kth, less);
+        uint32_t* dist = sh.dist;
+        const uint32_t nl = block_compact<T>(
+            nc, [&](uint32_t, uint32_t v) { return dist[v] < kth; }, [](uint32_t i) { return i; },
+            sh.pos, s);
+        block_compact<T>(nc, [&](uint32_t, uint32_t v) { return dist[v] == kth; },
+                         [](uint32_t i) { return i; }, sh.pos + nl, s);
+        const uint32_t N = next_pow2(m);
+        for (uint32_t i = threadIdx.x; i < N; i += T) {
+            if (i < m) {
+                const uint32_t ci = sh.pos[i];
+                sh.sorth[i] = ((uint64_t)dist[ci] << 32) | ci;
+            } else {
+                sh.sorth[i] = ~0ull;
+            }
+        }
+        __syncthreads();
+        block_bitonic_sort<T>(sh.sorth, N);
+        for (uint32_t i = threadIdx.x; i < m; i += T) sh.order[i] = (uint32_t)sh.sorth[i];
+        __syncthreads();
+        return m;
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+template <int T>
+__device__ void prepare_query(const SearchParams& p, Shared& sh, uint32_t q) {
+    const DevLevel& lv = p.l1;
+    const float* src = p.queries + (size_t)q * lv.d;
+    for (uint32_t i = threadIdx.x; i < lv.d; i += T) sh.qf[i] = __ldg(src + i);
+    __syncthreads();
+    if (lv.is_u8) {
+        // QuantizeEmbedding (scalar.hpp:76-94), packed into the device word layout
+        const uint32_t nw = lv.qw_hoff + lv.n_hblocks * 16;
+        for (uint32_t w = threadIdx.x; w < nw; w += T) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint32_t dim;
+                bool valid;
+                if (w < lv.qw_hoff) {
+                    dim = w * 4 + b;
+                    valid = dim < lv.dv;
+                } else {
+                    dim = lv.dv + (w - lv.qw_hoff) * 4 + b;
+                    valid = true;
+                }
+                uint32_t byte = 0;
+                if (valid) {
+                    const float v = __fmul_rn(__fsub_rn(sh.qf[dim], lv.base), lv.scale);
+                    const int r = (int)roundf(v);
+                    byte = r > 255 ? 255u : (r < 0 ? 0u : (uint32_t)r);
+                }
+                word |= byte << (8 * b);
+            }
+            sh.qw[w] = word;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool U8, int T>
+__global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ SearchParams p) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ Scalars s;
+    Shared sh;
+    sh.qf = reinterpret_cast<float*>(smem + p.smem_qf);
+    sh.qw = reinterpret_cast<uint32_t*>(smem + p.smem_qw);
+    sh.dist = reinterpret_cast<uint32_t*>(smem + p.smem_work);
+    sh.pos = sh.dist + p.work_cap;
+    sh.sortw = reinterpret_cast<uint64_t*>(smem + p.smem_work);
+    sh.hd = reinterpret_cast<float*>(smem + p.smem_heap);
+    sh.hid = reinterpret_cast<uint32_t*>(smem + p.smem_heap) + p.heap_cap;
+    sh.sorth = reinterpret_cast<uint64_t*>(smem + p.smem_heap);
+    sh.order = reinterpret_cast<uint32_t*>(smem + p.smem_order);
+
+    for (;;) {
+        if (threadIdx.x == 0) s.query = atomicAdd(p.queue, 1u);
+        __syncthreads();
+        const uint32_t q = s.query;
+        __syncthreads();
+        if (q >= p.nq) break;
+        const int filter = p.filter_of ? p.filter_of[q] : -1;
+        prepare_query<T>(p, sh, q);
+
+        uint32_t nvisit;
+        if (p.order) {
+            // caller-provided access order (PDXearch::SetClusterAccessOrder, searcher.hpp:48-54)
+            nvisit = p.nprobe < p.n_order ? p.nprobe : p.n_order;
+            for (uint32_t i = threadIdx.x; i < nvisit; i += T) sh.order[i] = __ldg(p.order + i);
+            __syncthreads();
+        } else if (p.is_tree && filter < 0) {
+            // PDXTreeIndex::Search (index.hpp:545-566): pruned F32 search over the meso
+            // clusters with k = nprobe returns the L1 clusters to visit, nearest first.
+            LevelOps<T, false> top(p, p.l0, sh, s, -1);
+            top.probe(p.top_nprobe);
+            const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
+            top.run(p.nprobe, nv0);
+            const uint32_t cnt = top.sort_heap(p.nprobe);
+            for (uint32_t i = threadIdx.x; i < cnt; i += T) sh.order[i] = (uint32_t)sh.sortw[i];
+            __syncthreads();
+            nvisit = cnt;
+        } else {
+            LevelOps<T, false> probe_ops(p, p.l1, sh, s, -1);
+            nvisit = probe_ops.probe(p.nprobe);
+        }
+
+        LevelOps<T, U8> ops(p, p.l1, sh, s, filter);
+        ops.run(p.k, nvisit);
+        const uint32_t cnt = ops.sort_heap(p.k);
+        uint32_t* oi = p.out_ids + (size_t)q * p.k;
+        float* od = p.out_dists + (size_t)q * p.k;
+        for (uint32_t i = threadIdx.x; i < p.k; i += T) {
+            if (i < cnt) {
+                const uint64_t e = sh.sortw[i];
+                oi[i] = (uint32_t)e;
+                od[i] = __uint_as_float((uint32_t)(e >> 32));
+            } else {
+                oi[i] = 0xFFFFFFFFu;
+                od[i] = __int_as_float(0x7f800000);
+            }
+        }
+        if (threadIdx.x == 0) p.out_counts[q] = cnt;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+template <bool U8, int T>
+static cudaError_t launch_t(const SearchParams& p, int grid, cudaStream_t st) {
+    auto kern = search_kernel<U8, T>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)p.smem_total);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, T, p.smem_total, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <bool U8, int T>
+static int occupancy_u(size_t smem) {
+    int blocks = 0;
+    cudaFuncSetAttribute(search_kernel<U8, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, search_kernel<U8, T>, T, smem);
+    return blocks;
+}
+template <int T>
+static int occupancy_t(bool u8, size_t smem) {
+    return u8 ? occupancy_u<true, T>(smem) : occupancy_u<false, T>(smem);
+}
+
+int search_occupancy(bool u8, int threads, size_t smem) {
+    switch (threads) {
+    case 128: return occupancy_t<128>(u8, smem);
+    case 256: return occupancy_t<256>(u8, smem);
+    case 512: return occupancy_t<512>(u8, smem);
+    default: return 0;
+    }
+}
+
+cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid, cudaStream_t st) {
+    switch (threads) {
+    case 128: return u8 ? launch_t<true, 128>(p, grid, st) : launch_t<false, 128>(p, grid, st);
+    case 256: return u8 ? launch_t<true, 256>(p, grid, st) : launch_t<false, 256>(p, grid, st);
+    case 512: return u8 ? launch_t<true, 512>(p, grid, st) : launch_t<false, 512>(p, grid, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace pdxg

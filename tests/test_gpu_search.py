@@ -1,0 +1,241 @@
+"""GPU parity tests: the CUDA search path (through the C ABI) against the reference's own results
+(golden fixtures) and against the oracle port on freshly generated indexes.
+
+Parity bar: on the same prepared (rotated) queries, distances are bit-identical and ids equal
+(as sets inside groups of tied distances) for every index type -- U8 and F32, pruning on and
+off, plain, fixed-order and filtered search. Raw queries additionally go through the GPU
+rotation, compared with the reference's BLAS rotation at FP32 tolerance (rtol 1e-5)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from pdx_b200 import compiled
+from pdx_b200.builder import GaussianMixture, build_index
+from pdx_b200.layout import IndexFile, Level, max_capacity, quantization_params, quantize
+from tests.helpers import assert_same, golden_cases, load_golden, recall
+
+pytestmark = pytest.mark.gpu
+CASES = [c["name"] for c in golden_cases()]
+
+
+@pytest.fixture(scope="module")
+def port_cls(built_oracle):
+    from oracle.oracle import Port
+    return Port
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_plain(name):
+    path, q, r, exp = load_golden(name)
+    ix = compiled.load_index(path)
+    ix.set_nprobe(exp["nprobe"])
+    ids, ds, cnt = ix.search_batch(r, exp["k"], transformed=True)
+    for i in range(len(r)):
+        assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], exp["plain_ids"][i], exp["plain_dists"][i],
+                    ctx=f"{name} q{i}")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_order_filtered_unpruned(name):
+    path, q, r, exp = load_golden(name)
+    ix = compiled.load_index(path)
+    k = exp["k"]
+    ix.set_nprobe(exp["nprobe"])
+    ids, ds, cnt = ix.search_with_order(r, k, np.array(exp["order"], np.uint32), transformed=True)
+    for i in range(len(r)):
+        assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], exp["order_ids"][i], exp["order_dists"][i],
+                    ctx=f"{name} order q{i}")
+    fids, fds, fcnt = ix.filtered_search_batch(r, k, [np.array(f, np.uint64) for f in exp["filters"]],
+                                               transformed=True)
+    for i in range(len(r)):
+        assert_same(fids[i, :fcnt[i]], fds[i, :fcnt[i]], exp["filt_ids"][i], exp["filt_dists"][i],
+                    ctx=f"{name} filtered q{i}")
+    ix.set_pruning_aggressiveness(1e30)
+    eids, eds, ecnt = ix.search_batch(r, k, transformed=True)
+    for i in range(len(r)):
+        assert_same(eids[i, :ecnt[i]], eds[i, :ecnt[i]], exp["exh_ids"][i], exp["exh_dists"][i],
+                    ctx=f"{name} unpruned q{i}")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_raw_queries(name):
+    path, q, r, exp = load_golden(name)
+    ix = compiled.load_index(path)
+    prepared = ix.prepare_queries(q)
+    np.testing.assert_allclose(prepared, r, rtol=1e-5, atol=1e-6)
+    ix.set_nprobe(exp["nprobe"])
+    ids, ds, cnt = ix.search_batch(q, exp["k"])
+    for i in range(len(q)):
+        assert recall(ids[i, :cnt[i]], exp["raw_ids"][i], exp["k"]) >= 0.9
+        common = set(ids[i, :cnt[i]].tolist()) & set(exp["raw_ids"][i])
+        for rid in common:
+            a = ds[i, list(ids[i, :cnt[i]]).index(rid)]
+            b = exp["raw_dists"][i][exp["raw_ids"][i].index(rid)]
+            assert abs(a - b) <= 1e-4 * max(abs(b), 1e-3) + 1e-5
+
+
+def _fresh(itype, d, n, nlist, nmeso=0, norm=False, seed=0, sigma=0.5, comps=16):
+    gm = GaussianMixture(d, comps, sigma, seed=seed + d, unit_norm=norm)
+    X = gm.sample(n, 0)
+    Q = gm.sample(24, 1)
+    f = build_index(X, itype, num_clusters=nlist, num_meso_clusters=nmeso, normalize=norm, seed=seed)
+    return f, X, Q
+
+
+def _compare_with_port(port_cls, f, Q, k, nprobes, threads=(256,)):
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        port = port_cls(p)
+        ix = compiled.load_index(p)
+        R = ix.prepare_queries(Q)
+        for nprobe in nprobes:
+            ix.set_nprobe(nprobe)
+            port.set_nprobe(nprobe)
+            for t in threads:
+                ix.set_threads_per_query(t)
+                ids, ds, cnt = ix.search_batch(R, k, transformed=True)
+                for i in range(len(R)):
+                    pi, pd = port.search(R[i], k, transformed=True)
+                    assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd,
+                                ctx=f"type={f.index_type} d={f.d} k={k} nprobe={nprobe} T={t} q{i}")
+        port.close()
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8", "pdx_tree_f32", "pdx_tree_u8"])
+@pytest.mark.parametrize("d", [3, 5, 63, 65, 127, 129, 200, 384])
+def test_fresh_vs_port_dims(port_cls, itype, d):
+    f, X, Q = _fresh(itype, d, 1500, 12, 3, norm=(d % 2 == 0), seed=1)
+    _compare_with_port(port_cls, f, Q, 10, (0, 4))
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8", "pdx_tree_f32", "pdx_tree_u8"])
+def test_fresh_vs_port_k_and_threads(port_cls, itype):
+    f, X, Q = _fresh(itype, 160, 3000, 20, 4, norm=True, seed=4)
+    for k in (1, 7, 100):
+        _compare_with_port(port_cls, f, Q, k, (0, 1, 6, 25), threads=(128, 256, 512))
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8", "pdx_tree_u8"])
+def test_large_d(port_cls, itype):
+    f, X, Q = _fresh(itype, 1024, 3000, 16, 4, norm=True, seed=7, sigma=0.25)
+    _compare_with_port(port_cls, f, Q, 20, (5,))
+
+
+def _manual_index(itype, d, sizes, seed=0):
+    """Index with exactly the given cluster sizes (0 allowed) from random data."""
+    rng = np.random.default_rng(seed)
+    n = sum(sizes)
+    X = rng.standard_normal((max(n, 1), d)).astype(np.float32)[:n]
+    rot = np.linalg.qr(rng.standard_normal((d, d)))[0].astype(np.float32)
+    R = (X.astype(np.float64) @ rot.astype(np.float64)).astype(np.float32)
+    is_u8 = itype in ("pdx_u8", "pdx_tree_u8")
+    base, scale = quantization_params(R) if n else (0.0, 1.0)
+    stored = quantize(R, base, scale) if is_u8 else R
+    embs, ids, cents = [], [], []
+    perm = rng.permutation(n).astype(np.uint32)
+    s = 0
+    for m in sizes:
+        sel = perm[s:s + m]
+        s += m
+        embs.append(np.ascontiguousarray(stored[sel]) if m else np.zeros((0, d), stored.dtype))
+        ids.append(sel)
+        cents.append(R[sel].mean(0) if m else rng.standard_normal(d).astype(np.float32))
+    cents = np.array(cents, np.float32)
+    l1 = Level(embs, ids, cents)
+    itype_id = {"pdx_f32": 0, "pdx_u8": 1, "pdx_tree_f32": 2, "pdx_tree_u8": 3}[itype]
+    l0 = None
+    if itype_id >= 2:
+        half = len(sizes) // 2
+        groups = [np.arange(half, dtype=np.uint32), np.arange(half, len(sizes), dtype=np.uint32)]
+        l0 = Level([cents[g] for g in groups], groups, np.array([cents[g].mean(0) for g in groups], np.float32))
+    return IndexFile(itype_id, rot, d, l1, l0, False, float(base), float(scale)), X
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8", "pdx_tree_f32", "pdx_tree_u8"])
+def test_edge_cluster_sizes(port_cls, itype):
+    f, X = _manual_index(itype, 72, [0, 1, 31, 33, 0, 5, 64, 257, 2, 0])
+    Q = np.random.default_rng(5).standard_normal((16, 72)).astype(np.float32)
+    _compare_with_port(port_cls, f, Q, 10, (0, 3, 11))
+    _compare_with_port(port_cls, f, Q, 500, (0,))  # k larger than the index
+
+
+def test_save_roundtrip_bytes():
+    for name in CASES:
+        path, *_ = load_golden(name)
+        ix = compiled.load_index(path)
+        with tempfile.TemporaryDirectory() as td:
+            out = os.path.join(td, "saved.pdx")
+            ix.save(out)
+            assert open(out, "rb").read() == open(path, "rb").read(), name
+
+
+def test_getters_match_file():
+    from pdx_b200.layout import read_index
+    for name in CASES:
+        path, *_ = load_golden(name)
+        f = read_index(open(path, "rb").read())
+        ix = compiled.load_index(path)
+        assert ix.get_num_dimensions() == f.d
+        assert ix.get_num_clusters() == f.l1.nclusters
+        for c in range(f.l1.nclusters):
+            assert ix.get_cluster_size(c) == f.l1.embeddings[c].shape[0]
+            np.testing.assert_array_equal(ix.get_cluster_row_ids(c), f.l1.row_ids[c])
+        assert ix.get_in_memory_size_in_bytes() > 0
+
+
+def test_batch_equals_single_queries():
+    path, q, r, exp = load_golden("tree_u8_d256")
+    ix = compiled.load_index(path)
+    ix.set_nprobe(exp["nprobe"])
+    ids, ds, cnt = ix.search_batch(q, exp["k"])
+    for i in range(len(q)):
+        si, sd = ix.search(q[i], exp["k"])
+        np.testing.assert_array_equal(si, ids[i, :cnt[i]])
+        np.testing.assert_array_equal(sd, ds[i, :cnt[i]])
+
+
+def test_filtered_mixed_batch(port_cls):
+    f, X, Q = _fresh("pdx_u8", 96, 4000, 24, seed=9)
+    rng = np.random.default_rng(3)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        port = port_cls(p)
+        ix = compiled.load_index(p)
+        R = ix.prepare_queries(Q)
+        lists = []
+        for i in range(len(Q)):
+            if i % 3 == 0:
+                lists.append(None)
+            else:
+                sel = float(np.exp(rng.uniform(np.log(0.001), np.log(0.5))))
+                lists.append(np.sort(rng.choice(4000, max(1, int(4000 * sel)), replace=False)).astype(np.uint64))
+        for nprobe in (0, 5):
+            ix.set_nprobe(nprobe)
+            port.set_nprobe(nprobe)
+            ids, ds, cnt = ix.filtered_search_batch(R, 10, lists, transformed=True)
+            for i in range(len(Q)):
+                if lists[i] is None:
+                    pi, pd = port.search(R[i], 10, transformed=True)
+                else:
+                    pi, pd = port.filtered_search(R[i], 10, lists[i], transformed=True)
+                    assert set(ids[i, :cnt[i]].tolist()) <= set(lists[i].tolist())
+                assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd, ctx=f"filtered nprobe={nprobe} q{i}")
+        port.close()
+
+
+def test_filtered_edge_cases():
+    path, q, r, exp = load_golden("f32_d64")
+    ix = compiled.load_index(path)
+    ix.set_nprobe(0)
+    ids, ds = ix.filtered_search(q[0], 10, np.array([], np.uint64))
+    assert len(ids) == 0
+    ids, ds = ix.filtered_search(q[0], 10, np.array([17], np.uint64))
+    assert ids.tolist() == [17]
+    all_rows = np.arange(1200, dtype=np.uint64)
+    a = ix.filtered_search(q[1], 10, all_rows)
+    b = ix.search(q[1], 10)
+    np.testing.assert_array_equal(a[1], b[1])
