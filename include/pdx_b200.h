@@ -43,6 +43,9 @@ typedef struct pdxg_index pdxg_index;
 #define PDXG_QUERY_TRANSFORMED 1u /* queries are already normalized + rotated: the reference's
                                      Search(query, k, is_query_transformed = true),
                                      searcher.hpp:596-613 */
+#define PDXG_COLLECT_STATS 2u     /* count the index bytes the search algorithm reads (centroid
+                                     probes, Start scans, warmup steps, survivor gathers);
+                                     read them back with pdxg_get_stats */
 
 /* Last error message of the calling thread (never NULL). */
 const char* pdxg_last_error(void);
@@ -120,6 +123,14 @@ uint64_t pdxg_num_embeddings(const pdxg_index* index);
 /* Rotated (normalized when the index is) queries, as the search sees them: the reference's
  * ADSamplingPruner::PreprocessQuery (adsampling.hpp:100-113) on nq host queries. */
 int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, float* out);
+
+/* Counters of the last search launched with PDXG_COLLECT_STATS (synchronizes the index's
+ * stream): out[0] index bytes read by the algorithm, out[1] clusters visited, out[2] vectors
+ * that reached the heap merge, out[3..8] the bytes of out[0] by phase (tree top-level search,
+ * Start scans, warmup steps, survivor horizontal blocks, survivor vertical dims, centroid
+ * probe). No counterpart in the reference (its profiler times phases, profiler.hpp:36-320);
+ * used for the roofline accounting. */
+int pdxg_get_stats(pdxg_index* index, uint64_t out[9]);
 
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);

@@ -37,15 +37,17 @@ class GaussianMixture:
         self.seed = seed
 
     def sample(self, n: int, stream: int) -> np.ndarray:
-        rng = np.random.default_rng([self.seed, stream])
-        labels = rng.integers(0, self.centres.shape[0], n)
+        """n points of sample stream `stream`; sample(m, s) is a prefix of sample(n, s), m <= n."""
         out = np.empty((n, self.d), dtype=np.float32)
         chunk = 1 << 16
-        for s in range(0, n, chunk):
+        for c, s in enumerate(range(0, n, chunk)):
             e = min(n, s + chunk)
-            x = rng.standard_normal((e - s, self.d), dtype=np.float32)
+            labels = np.random.default_rng([self.seed, stream, c, 0]).integers(
+                0, self.centres.shape[0], e - s)
+            x = np.random.default_rng([self.seed, stream, c, 1]).standard_normal(
+                (e - s, self.d), dtype=np.float32)
             x *= self.sigma
-            x += self.centres[labels[s:e]]
+            x += self.centres[labels]
             if self.unit_norm:
                 x /= np.linalg.norm(x, axis=1, keepdims=True).astype(np.float32)
             out[s:e] = x
@@ -173,7 +175,7 @@ def build_index(data: np.ndarray, index_type: str = "pdx_f32", num_clusters: int
     if is_u8:
         base, scale = quantization_params(rot)
     cents, assign = kmeans(rot, num_clusters, kmeans_iters, seed, device)
-    stored = quantize(rot, base, scale) if is_u8 else rot
+    stored = _quantize(rot, base, scale, device) if is_u8 else rot
     row_ids = np.arange(n, dtype=np.uint32)
     embs, ids = _split_by_assignment(stored, row_ids, assign, num_clusters)
     l1 = Level(embs, ids, cents)
@@ -186,6 +188,24 @@ def build_index(data: np.ndarray, index_type: str = "pdx_f32", num_clusters: int
         e0, i0 = _split_by_assignment(cents, np.arange(num_clusters, dtype=np.uint32), a0, n0)
         l0 = Level(e0, i0, c0)
     return IndexFile(itype, rotation, d, l1, l0, bool(normalize), float(base), float(scale))
+
+
+def _quantize(x: np.ndarray, base: float, scale: float, device: Optional[str]) -> np.ndarray:
+    """quantize() of layout.py, chunked on the GPU when a device is given (same float32 steps,
+    round half away from zero)."""
+    if device is None:
+        return quantize(x, base, scale)
+    import torch
+    out = np.empty(x.shape, dtype=np.uint8)
+    b = torch.tensor(np.float32(base), device=device)
+    s = torch.tensor(np.float32(scale), device=device)
+    step = 1 << 17
+    for i in range(0, x.shape[0], step):
+        v = (torch.from_numpy(x[i:i + step]).to(device) - b) * s
+        v64 = v.double()
+        r = torch.trunc(v64 + torch.copysign(torch.full_like(v64, 0.5), v64))
+        out[i:i + step] = r.clamp(0, 255).to(torch.uint8).cpu().numpy()
+    return out
 
 
 def _rotate(x: np.ndarray, rotation: np.ndarray, device: Optional[str]) -> np.ndarray:

@@ -24,6 +24,7 @@ _lib = None
 PDXG_OK = 0
 PDXG_ERR_INVALID_ARGUMENT = 1
 PDXG_QUERY_TRANSFORMED = 1
+PDXG_COLLECT_STATS = 2
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -69,6 +70,7 @@ def library() -> C.CDLL:
         fn("pdxg_in_memory_size_in_bytes", C.c_uint64, vp)
         fn("pdxg_num_embeddings", C.c_uint64, vp)
         fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
+        fn("pdxg_get_stats", C.c_int, vp, _u64p)
         _lib = lib
     return _lib
 
@@ -274,6 +276,22 @@ class PDXIndex:
         out = np.empty_like(Q)
         _check(library().pdxg_prepare_queries(h.ptr, Q, Q.shape[0], out))
         return out
+
+    def search_device(self, queries_ptr: int, nq: int, knn: int, ids_ptr: int, dists_ptr: int,
+                      counts_ptr: int, stream: int = 0, transformed: bool = False,
+                      stats: bool = False) -> None:
+        """Enqueues a search on GPU-resident buffers (raw device pointers) on `stream`."""
+        flags = (PDXG_QUERY_TRANSFORMED if transformed else 0) | (PDXG_COLLECT_STATS if stats else 0)
+        _check(library().pdxg_search_device(self._handle().ptr, C.c_void_p(queries_ptr), nq, knn,
+                                            flags, C.c_void_p(ids_ptr), C.c_void_p(dists_ptr),
+                                            C.c_void_p(counts_ptr), C.c_void_p(stream)))
+
+    def last_stats(self) -> dict:
+        out = np.zeros(9, np.uint64)
+        _check(library().pdxg_get_stats(self._handle().ptr, out))
+        names = ["top_level", "start", "warmup", "survivor_horizontal", "survivor_vertical", "probe"]
+        return {"bytes": int(out[0]), "clusters_visited": int(out[1]), "merged": int(out[2]),
+                "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])}}
 
     def set_pruning_aggressiveness(self, epsilon0: float) -> None:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))

@@ -68,6 +68,10 @@ struct SearchParams {
     float* out_dists;            // [nq x k]
     uint32_t* out_counts;        // [nq]
     uint32_t* queue;             // work counter (zeroed before launch)
+    unsigned long long* stats;   // optional [9]: [0] index bytes the algorithm reads, [1] clusters
+                                 // visited, [2] vectors reaching the merge, [3..8] bytes by phase:
+                                 // top-level search, Start, warmup, survivor horizontal blocks,
+                                 // survivor vertical dims, centroid probe
     // shared-memory carve-up (bytes), computed by the host
     uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_total;
     uint32_t work_cap;           // entries of the dist / pos work arrays (power of two)

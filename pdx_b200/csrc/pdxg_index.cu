@@ -247,6 +247,7 @@ struct Workspace {
     uint64_t pass_cap = 0;
     int32_t* d_filter_of = nullptr;
     uint32_t fo_cap = 0;
+    unsigned long long* d_stats = nullptr;
 };
 
 }  // namespace
@@ -275,6 +276,7 @@ struct pdxg_index {
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
     cudaStream_t stream = nullptr;
+    cudaStream_t stats_stream = nullptr;
     Workspace ws;
     std::mutex mu;
 };
@@ -344,6 +346,7 @@ void free_index(pdxg_index* ix) {
     cudaFree(w.d_sel);
     cudaFree(w.d_pass);
     cudaFree(w.d_filter_of);
+    cudaFree(w.d_stats);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
 }
@@ -647,6 +650,13 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     L.p.out_dists = dists;
     L.p.out_counts = counts;
     L.p.queue = ix->ws.d_queue;
+    L.p.stats = nullptr;
+    if (flags & PDXG_COLLECT_STATS) {
+        if (!ix->ws.d_stats) PDXG_CUDA(cudaMalloc(&ix->ws.d_stats, 9 * sizeof(unsigned long long)));
+        PDXG_CUDA(cudaMemsetAsync(ix->ws.d_stats, 0, 9 * sizeof(unsigned long long), st));
+        L.p.stats = ix->ws.d_stats;
+        ix->stats_stream = st;
+    }
     PDXG_CUDA(cudaMemsetAsync(ix->ws.d_queue, 0, sizeof(uint32_t), st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     return PDXG_OK;
@@ -873,6 +883,19 @@ int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, floa
                                      ix->ws.d_norms, ix->ws.d_rq, st));
     PDXG_CUDA(cudaMemcpyAsync(out, ix->ws.d_rq, sizeof(float) * nq * ix->d, cudaMemcpyDeviceToHost, st));
     PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+int pdxg_get_stats(pdxg_index* ix, uint64_t out[9]) {
+    if (int rc = check_index(ix)) return rc;
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (!ix->ws.d_stats) return fail(PDXG_ERR_INVALID_ARGUMENT, "no search ran with PDXG_COLLECT_STATS");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    PDXG_CUDA(cudaStreamSynchronize(ix->stats_stream ? ix->stats_stream : ix->stream));
+    unsigned long long h[9];
+    PDXG_CUDA(cudaMemcpy(h, ix->ws.d_stats, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 9; ++i) out[i] = h[i];
     return PDXG_OK;
 }
 

@@ -54,7 +54,13 @@ struct Scalars {
     float top;
     uint32_t query;
     uint32_t n_order;
+    unsigned long long bytes[6];  // algorithmic bytes of the current query by phase (stats only)
+    unsigned long long visits;
+    unsigned long long merged;
 };
+
+// Phases of the algorithmic-byte accounting (stats[3 + phase]).
+enum Phase { kTopLevel = 0, kStart = 1, kWarmup = 2, kSurvivorH = 3, kSurvivorV = 4, kProbe = 5 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
@@ -237,11 +243,12 @@ struct LevelOps {
     const DevLevel& lv;
     Shared& sh;
     Scalars& s;
-    int filter;  // -1 = unfiltered
+    int filter;      // -1 = unfiltered
+    bool top_level;  // the tree's meso-cluster search
 
     __device__ LevelOps(const SearchParams& p_, const DevLevel& lv_, Shared& sh_, Scalars& s_,
-                        int filter_)
-        : p(p_), lv(lv_), sh(sh_), s(s_), filter(filter_) {}
+                        int filter_, bool top_level_ = false)
+        : p(p_), lv(lv_), sh(sh_), s(s_), filter(filter_), top_level(top_level_) {}
 
     __device__ __forceinline__ const uint32_t* vert(const DevCluster& c) const {
         return reinterpret_cast<const uint32_t*>(p.arena + c.vert_off);
@@ -272,6 +279,12 @@ struct LevelOps {
         const uint32_t* bits = p.sel_bits + (size_t)filter * lv.sel_words + c.sel_word;
         return (__ldg(bits + (v >> 5)) >> (v & 31)) & 1u;
     }
+    // Algorithmic-traffic accounting (only when p.stats is set; values are block-uniform).
+    __device__ __forceinline__ void count_bytes(unsigned long long b, Phase ph) const {
+        if (p.stats && threadIdx.x == 0) s.bytes[top_level ? kTopLevel : ph] += b;
+    }
+    static constexpr uint32_t kElem = U8 ? 1u : 4u;
+
     __device__ __forceinline__ uint32_t mask_raw() const {
         return u8 ? kMaskU8 : __float_as_uint(PDXG_MASK_F32);
     }
@@ -470,6 +483,7 @@ struct LevelOps {
 
     // searcher.hpp:217-281
     __device__ void start(const DevCluster& c, uint32_t k) {
+        count_bytes((unsigned long long)c.n * lv.d * kElem, kStart);
         zero_dist(c.n);
         vertical_all(c, 0, lv.dv, false, 0);
         __syncthreads();
@@ -485,6 +499,9 @@ struct LevelOps {
         const uint32_t nsel = block_compact<T>(
             c.n, [&](uint32_t i, uint32_t) { return selected(c, i); }, [](uint32_t i) { return i; },
             sh.pos, s);
+        count_bytes((unsigned long long)nsel * lv.dh * kElem +
+                    (unsigned long long)((__fdiv_rn((float)passing, (float)c.n) > (1.0f - kSelectivity)) ? c.n : nsel) *
+                        lv.dv * kElem, kStart);
         for (uint32_t b = 0; b < lv.n_hblocks; ++b) horizontal(c, b, nsel, false);
         const float pct = __fdiv_rn((float)passing, (float)c.n);
         if (pct > (1.0f - kSelectivity)) {
@@ -523,6 +540,7 @@ struct LevelOps {
                 uint32_t last = cur + c_fetch_sizes[step < kNumFetchSizes ? step : kNumFetchSizes - 1];
                 if (last > lv.dv) last = lv.dv;
                 const uint32_t thr = thr_raw(last);
+                count_bytes((unsigned long long)n * (last - cur) * kElem, kWarmup);
                 n_pruned = vertical_all(c, cur, last, true, thr);
                 cur = last;
                 ++step;
@@ -538,6 +556,7 @@ struct LevelOps {
             [](uint32_t i) { return i; }, sh.pos, s);
         uint32_t cur_v = cur, cur_h = 0;
         while (lv.dh && nsurv && cur_h < lv.dh) {
+            count_bytes((unsigned long long)nsurv * kHDim * kElem, kSurvivorH);
             horizontal(c, cur_h / kHDim, nsurv, false);
             cur_h += kHDim;
             cur += kHDim;
@@ -550,6 +569,7 @@ struct LevelOps {
         while (nsurv && cur_v < lv.dv) {
             uint32_t last = cur_v + kHDim;
             if (last > lv.dv) last = lv.dv;
+            count_bytes((unsigned long long)nsurv * (last - cur_v) * kElem, kSurvivorV);
             vertical_pos(c, cur_v, last, nsurv);
             cur = (cur + kHDim < lv.d) ? cur + kHDim : lv.d;
             cur_v = last;
@@ -560,6 +580,7 @@ struct LevelOps {
                 [&](uint32_t i) { return pos[i]; }, sh.pos, s);
             if (cur == lv.d) break;
         }
+        if (p.stats && threadIdx.x == 0) s.merged += nsurv;
         // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, survivor order.
         if (nsurv) {
             const uint32_t* idp = ids(c);
@@ -628,6 +649,7 @@ struct LevelOps {
                 if (passing == 0) continue;
             }
             if (c.n == 0) continue;
+            if (p.stats && threadIdx.x == 0) s.visits += 1;
             if (s.hsize < k) {
                 if (filter >= 0)
                     filtered_start(c, k, passing);
@@ -656,6 +678,7 @@ struct LevelOps {
     // Probe order over the level's centroids: nearest `nprobe` sorted ascending into sh.order.
     __device__ uint32_t probe(uint32_t nprobe) {
         const uint32_t nc = lv.nclusters;
+        count_bytes((unsigned long long)nc * lv.d * 4u, kProbe);
         const uint32_t lane = lane_id(), sub = lane & 7;
         for (uint32_t base = 0; base < nc; base += T / 8) {
             const uint32_t cidx = base + (threadIdx.x >> 3);
@@ -749,6 +772,11 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         const uint32_t q = s.query;
         __syncthreads();
         if (q >= p.nq) break;
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 6; ++i) s.bytes[i] = 0;
+            s.visits = 0;
+            s.merged = 0;
+        }
         const int filter = p.filter_of ? p.filter_of[q] : -1;
         prepare_query<T>(p, sh, q);
 
@@ -761,7 +789,7 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         } else if (p.is_tree && filter < 0) {
             // PDXTreeIndex::Search (index.hpp:545-566): pruned F32 search over the meso
             // clusters with k = nprobe returns the L1 clusters to visit, nearest first.
-            LevelOps<T, false> top(p, p.l0, sh, s, -1);
+            LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
             top.probe(p.top_nprobe);
             const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
             top.run(p.nprobe, nv0);
@@ -789,7 +817,19 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
                 od[i] = __int_as_float(0x7f800000);
             }
         }
-        if (threadIdx.x == 0) p.out_counts[q] = cnt;
+        if (threadIdx.x == 0) {
+            p.out_counts[q] = cnt;
+            if (p.stats) {
+                unsigned long long tot = 0;
+                for (int i = 0; i < 6; ++i) {
+                    tot += s.bytes[i];
+                    atomicAdd(p.stats + 3 + i, s.bytes[i]);
+                }
+                atomicAdd(p.stats, tot);
+                atomicAdd(p.stats + 1, s.visits);
+                atomicAdd(p.stats + 2, s.merged);
+            }
+        }
         __syncthreads();
     }
 }
