@@ -132,6 +132,33 @@ int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, f
  * used for the roofline accounting. */
 int pdxg_get_stats(pdxg_index* index, uint64_t out[9]);
 
+/* Size of the fixed scratch array behind pdxg_search_device_noalloc, per GPU. */
+#define PDXG_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/* Allocation-free variant of pdxg_search_device, for callers that must not have the library
+ * call cudaMalloc: hosts whose framework already owns the GPU's memory through its own pool,
+ * serving loops that cannot afford the device-wide synchronisation cudaMalloc/cudaFree may
+ * cause, plugins running under an allocation policy they do not control. It has no
+ * counterpart in the reference (whose CPU search allocates per call, searcher.hpp:601-653).
+ *
+ * Same arguments and results as pdxg_search_device (all pointers GPU memory; NULL stream = the
+ * index's own stream), but the scratch -- work counter, query norms, rotated queries -- comes
+ * from one fixed array of PDXG_NOALLOC_SCRATCH_BYTES compiled into the library; every GPU that
+ * loads the library holds it until the process exits. Limit: 512 + 4*nq + 4*nq*d bytes must
+ * fit (about 2,000 queries at d = 1024); larger batches fail with PDXG_ERR_CAPACITY, and with
+ * PDXG_QUERY_TRANSFORMED only the work counter is used, so any nq fits. PDXG_COLLECT_STATS is
+ * rejected. The first call on a device looks up the array's device address (with that device
+ * current); make that first call before any stream capture. All calls share the one array and
+ * it keeps the previous call's contents: calls whose work overlaps on the GPU (different
+ * streams, or different indexes on the same GPU) race on it and must be serialised by the
+ * caller. */
+int pdxg_search_device_noalloc(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k,
+                               uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts,
+                               void* stream);
+
+/* PDXG_NOALLOC_SCRATCH_BYTES as built into the library. */
+uint64_t pdxg_noalloc_scratch_bytes(void);
+
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);
 

@@ -662,6 +662,44 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     return PDXG_OK;
 }
 
+}  // namespace
+
+// Search on caller-provided workspace: never allocates. `norms` needs nq floats, `rotated`
+// nq * d floats (both unused with PDXG_QUERY_TRANSFORMED), `queue` one u32.
+int pdxg_search_on_workspace(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k,
+                             uint32_t flags, float* norms, float* rotated, uint32_t* queue,
+                             uint32_t* ids, float* dists, uint32_t* counts, cudaStream_t st) {
+    if (nq == 0) return PDXG_OK;
+    if (k == 0) {
+        PDXG_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, st));
+        return PDXG_OK;
+    }
+    const float* qp = q;
+    if (!(flags & PDXG_QUERY_TRANSFORMED)) {
+        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, norms, rotated, st));
+        qp = rotated;
+    }
+    Launch L;
+    int rc = plan_search(ix, nq, k, 0, false, L);
+    if (rc) return rc;
+    L.p.queries = qp;
+    L.p.out_ids = ids;
+    L.p.out_dists = dists;
+    L.p.out_counts = counts;
+    L.p.queue = queue;
+    PDXG_CUDA(cudaMemsetAsync(queue, 0, sizeof(uint32_t), st));
+    PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
+    return PDXG_OK;
+}
+
+int pdxg_index_device(const pdxg_index* ix) { return ix->device; }
+uint32_t pdxg_index_dims(const pdxg_index* ix) { return ix->d; }
+std::mutex& pdxg_index_mutex(pdxg_index* ix) { return ix->mu; }
+cudaStream_t pdxg_index_stream(pdxg_index* ix) { return ix->stream; }
+int pdxg_set_error(int code, const char* msg) { return fail(code, msg); }
+
+namespace {
+
 int check_index(const pdxg_index* ix) {
     if (!ix) return fail(PDXG_ERR_INVALID_ARGUMENT, "index is NULL");
     return PDXG_OK;
