@@ -427,7 +427,8 @@ def main():
                          "kernel": "search_kernel", "kernel_ms": round(kern_ms, 3),
                          "algorithmic_bytes_per_launch": stats["bytes"], "peak_source": peak_src,
                          "clusters_visited": stats["clusters_visited"],
-                         "bytes_by_phase": stats["bytes_by_phase"]},
+                         "bytes_by_phase": stats["bytes_by_phase"],
+                         "cycles_by_phase": stats["cycles_by_phase"]},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * d * 4,

@@ -128,9 +128,10 @@ int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, f
  * stream): out[0] index bytes read by the algorithm, out[1] clusters visited, out[2] vectors
  * that reached the heap merge, out[3..8] the bytes of out[0] by phase (tree top-level search,
  * Start scans, warmup steps, survivor horizontal blocks, survivor vertical dims, centroid
- * probe). No counterpart in the reference (its profiler times phases, profiler.hpp:36-320);
+ * probe), out[9..11] SM cycles spent per query in the top-level search, in Start, and in
+ * the rest of the scan. No counterpart in the reference (its profiler times phases, profiler.hpp:36-320);
  * used for the roofline accounting. */
-int pdxg_get_stats(pdxg_index* index, uint64_t out[9]);
+int pdxg_get_stats(pdxg_index* index, uint64_t out[12]);
 
 /* Size of the fixed scratch array behind pdxg_search_device_noalloc, per GPU. */
 #define PDXG_NOALLOC_SCRATCH_BYTES (8u << 20)
@@ -158,6 +159,13 @@ int pdxg_search_device_noalloc(pdxg_index* index, const float* queries, uint32_t
 
 /* PDXG_NOALLOC_SCRATCH_BYTES as built into the library. */
 uint64_t pdxg_noalloc_scratch_bytes(void);
+
+/* Engine tuning, tree indexes: how the top-level (meso-cluster) search runs. 0 = automatic
+ * (batched for batches of 32+ queries), 1 = inside each query's search CTA, 2 = batched: a probe
+ * kernel and a partials kernel compute, for all queries at once, the exact values the
+ * top-level decisions depend on, and each query replays PDXTreeIndex::Search's decisions
+ * (index.hpp:545-566) on them. Results are identical in every mode. */
+int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
 
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);

@@ -52,6 +52,7 @@ def library() -> C.CDLL:
         fn("pdxg_set_nprobe", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_pruning_aggressiveness", C.c_int, vp, C.c_float)
         fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
+        fn("pdxg_set_top_level_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
         fn("pdxg_search_with_order", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u32p, C.c_uint32,
@@ -287,14 +288,19 @@ class PDXIndex:
                                             C.c_void_p(counts_ptr), C.c_void_p(stream)))
 
     def last_stats(self) -> dict:
-        out = np.zeros(9, np.uint64)
+        out = np.zeros(12, np.uint64)
         _check(library().pdxg_get_stats(self._handle().ptr, out))
         names = ["top_level", "start", "warmup", "survivor_horizontal", "survivor_vertical", "probe"]
         return {"bytes": int(out[0]), "clusters_visited": int(out[1]), "merged": int(out[2]),
-                "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])}}
+                "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])},
+                "cycles_by_phase": {n: int(v) for n, v in zip(["top_level", "start", "rest"], out[9:12])}}
 
     def set_pruning_aggressiveness(self, epsilon0: float) -> None:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))
+
+    def set_top_level_mode(self, mode: int) -> None:
+        """Tree indexes: 0 automatic, 1 per-query top-level search, 2 batched two-phase."""
+        _check(library().pdxg_set_top_level_mode(self._handle().ptr, int(mode)))
 
     def set_threads_per_query(self, threads: int) -> None:
         _check(library().pdxg_set_threads_per_query(self._handle().ptr, int(threads)))

@@ -68,15 +68,46 @@ struct SearchParams {
     float* out_dists;            // [nq x k]
     uint32_t* out_counts;        // [nq]
     uint32_t* queue;             // work counter (zeroed before launch)
-    unsigned long long* stats;   // optional [9]: [0] index bytes the algorithm reads, [1] clusters
+    unsigned long long* stats;   // optional [12]: [0] index bytes the algorithm reads, [1] clusters
                                  // visited, [2] vectors reaching the merge, [3..8] bytes by phase:
                                  // top-level search, Start, warmup, survivor horizontal blocks,
-                                 // survivor vertical dims, centroid probe
+                                 // survivor vertical dims, centroid probe; [9..11] SM cycles
+                                 // in the top-level search, in L1 Start, in the rest
+    // tree top level, batched form (pdxg_toplevel.cu): each query's L1 visit order
+    const uint32_t* q_order;        // [nq x q_order_stride]
+    const uint32_t* q_order_count;  // [nq]
+    uint32_t q_order_stride;
     // shared-memory carve-up (bytes), computed by the host
     uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_total;
-    uint32_t work_cap;           // entries of the dist / pos work arrays (power of two)
+    uint32_t work_cap;           // entries of the dist / pos work arrays (multiple of 32, >= heap_cap)
     uint32_t heap_cap;           // entries of the heap arrays (power of two)
     uint32_t order_cap;          // entries of the cluster order list
+};
+
+// The batched top-level stage (pdxg_toplevel.cu).
+struct TopLevelParams {
+    const uint8_t* arena;
+    DevLevel l0;
+    const float* queries;                 // prepared queries [nq x d]
+    uint32_t nq;
+    uint32_t top;                         // meso clusters probed per query
+    uint32_t nvals;                       // values per (query, vector): n_ckpt + l0.n_hblocks
+    uint32_t n_ckpt;
+    uint32_t ckpt[kNumFetchSizes + 1];    // cumulative warmup boundaries, capped at d_v
+    unsigned long long per_query_floats;  // partial-value budget of one query
+    uint32_t* order;                      // [nq x top] meso ids, nearest first
+    unsigned long long* offsets;          // [nq x top] float offsets into vals
+    uint32_t* lists;                      // [n0 x nq] entries q * top + rank
+    uint32_t* list_count;                 // [n0]
+    float* vals;
+    uint32_t n0_cap;                      // dist/pos entries in the probe's shared memory
+    uint32_t smem_dist, smem_sort, smem_total;
+    // replay (warp per query)
+    const float* ratios;
+    uint32_t k1;                          // L1 clusters to return per query (the L1 nprobe)
+    uint32_t* l1_order;                   // [nq x k1]
+    uint32_t* l1_count;                   // [nq]
+    uint32_t r_dist_cap, r_sort_cap, r_heap_cap, r_warp_bytes;
 };
 
 }  // namespace pdxg

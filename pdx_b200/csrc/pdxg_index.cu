@@ -23,6 +23,7 @@ cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid,
 int search_occupancy(bool u8, int threads, size_t smem);
 cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, const float* rotation,
                                    bool normalize, float* norms_ws, float* out, cudaStream_t st);
+cudaError_t launch_top_level(const TopLevelParams& tp, cudaStream_t st);
 }  // namespace pdxg
 
 using namespace pdxg;
@@ -248,6 +249,21 @@ struct Workspace {
     int32_t* d_filter_of = nullptr;
     uint32_t fo_cap = 0;
     unsigned long long* d_stats = nullptr;
+    // batched tree top level
+    uint32_t* d_top_order = nullptr;
+    uint64_t top_order_cap = 0;
+    unsigned long long* d_top_off = nullptr;
+    uint64_t top_off_cap = 0;
+    uint32_t* d_top_lists = nullptr;
+    uint64_t top_lists_cap = 0;
+    uint32_t* d_top_count = nullptr;
+    uint64_t top_count_cap = 0;
+    float* d_top_vals = nullptr;
+    uint64_t top_vals_cap = 0;
+    uint32_t* d_l1_order = nullptr;
+    uint64_t l1_order_cap = 0;
+    uint32_t* d_l1_count = nullptr;
+    uint64_t l1_count_cap = 0;
 };
 
 }  // namespace
@@ -272,6 +288,7 @@ struct pdxg_index {
     float eps0 = 1.5f;
     uint32_t nprobe = 0;
     uint32_t threads = 0;
+    uint32_t top_mode = 0;  // tree top level: 0 auto, 1 fused per query, 2 batched two-phase
     int num_sms = 0;
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
@@ -347,6 +364,13 @@ void free_index(pdxg_index* ix) {
     cudaFree(w.d_pass);
     cudaFree(w.d_filter_of);
     cudaFree(w.d_stats);
+    cudaFree(w.d_top_order);
+    cudaFree(w.d_top_off);
+    cudaFree(w.d_top_lists);
+    cudaFree(w.d_top_count);
+    cudaFree(w.d_top_vals);
+    cudaFree(w.d_l1_order);
+    cudaFree(w.d_l1_count);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
 }
@@ -562,7 +586,9 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
     uint32_t work = std::max({p.l1.max_n, heap_cap, 32u});
     if (!ix->tree || any_filter) work = std::max(work, n1);
     if (ix->tree) work = std::max({work, p.l0.max_n, p.l0.nclusters});
-    const uint32_t work_cap = next_pow2(work);
+    // dist/pos need max cluster size (or centroid count for a probe); sorts viewing the region as
+    // u64 need at most heap_cap (a power of two) entries, so no power-of-two padding here
+    const uint32_t work_cap = (work + 31) / 32 * 32;
     const uint32_t order_cap = std::max({np_flat, top, n_order, 1u});
     uint32_t off = 0;
     p.smem_qf = off;
@@ -620,6 +646,92 @@ int ensure_ws(pdxg_index* ix, uint32_t nq, uint32_t k) {
     return PDXG_OK;
 }
 
+// Warmup checkpoints: cumulative DIMENSIONS_FETCHING_SIZES capped at d_v (common.hpp:47-49).
+uint32_t warmup_checkpoints(uint32_t dv, uint32_t* out) {
+    static const uint32_t sizes[kNumFetchSizes] = {16,  16,  32,  32,  32,   32,   64,
+                                                   64,  64,  64,  128, 128,  128,  128,
+                                                   256, 256, 512, 1024, 2048, 16384};
+    uint32_t n = 0, cur = 0, step = 0;
+    while (cur < dv && n < (uint32_t)kNumFetchSizes) {
+        uint32_t last = cur + sizes[step < (uint32_t)kNumFetchSizes ? step : kNumFetchSizes - 1];
+        if (last > dv) last = dv;
+        out[n++] = last;
+        cur = last;
+        ++step;
+    }
+    return n;
+}
+
+// Batched tree top level (pdxg_toplevel.cu): fills L.p.top_* on success; leaves them NULL (the
+// search kernel then runs the fused per-query top level) when the mode or the batch says so.
+int run_top_level(pdxg_index* ix, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+    L.p.q_order = nullptr;
+    L.p.q_order_count = nullptr;
+    if (ix->top_mode == 1 || (ix->top_mode == 0 && nq < 32)) return PDXG_OK;
+    const HostLevel& l0 = ix->l0;
+    const uint32_t n0 = (uint32_t)l0.fc.size();
+    const uint32_t top = std::min(L.p.top_nprobe, n0);
+    if (top == 0) return PDXG_OK;
+    TopLevelParams tp{};
+    tp.arena = ix->arena;
+    tp.l0 = L.p.l0;
+    tp.queries = qp;
+    tp.nq = nq;
+    tp.top = top;
+    tp.n_ckpt = warmup_checkpoints(ix->dv, tp.ckpt);
+    tp.ckpt[tp.n_ckpt] = 0xFFFFFFFFu;
+    tp.nvals = tp.n_ckpt + l0.n_hblocks;
+    std::vector<uint32_t> sizes(l0.n.begin(), l0.n.end());
+    std::sort(sizes.begin(), sizes.end(), std::greater<uint32_t>());
+    uint64_t budget = 0;
+    for (uint32_t i = 0; i < top; ++i) budget += sizes[i];
+    tp.per_query_floats = budget * tp.nvals;
+    const uint64_t vals = (uint64_t)nq * tp.per_query_floats;
+    if (ix->top_mode == 0 && vals * 4 > (8ull << 30)) return PDXG_OK;  // keep workspaces bounded
+    Workspace& w = ix->ws;
+    int rc;
+    if ((rc = dev_grow(w.d_top_order, w.top_order_cap, (uint64_t)nq * top))) return rc;
+    if ((rc = dev_grow(w.d_top_off, w.top_off_cap, (uint64_t)nq * top))) return rc;
+    if ((rc = dev_grow(w.d_top_lists, w.top_lists_cap, (uint64_t)n0 * nq))) return rc;
+    if ((rc = dev_grow(w.d_top_count, w.top_count_cap, n0))) return rc;
+    if ((rc = dev_grow(w.d_top_vals, w.top_vals_cap, std::max<uint64_t>(vals, 1)))) return rc;
+    tp.order = w.d_top_order;
+    tp.offsets = w.d_top_off;
+    tp.lists = w.d_top_lists;
+    tp.list_count = w.d_top_count;
+    tp.vals = w.d_top_vals;
+    tp.n0_cap = (n0 + 31) / 32 * 32;
+    uint32_t pw = 1;
+    while (pw < top) pw <<= 1;
+    tp.smem_dist = (uint32_t)align_up((uint64_t)ix->d * 4, 16);
+    tp.smem_sort = tp.smem_dist + tp.n0_cap * 8;
+    tp.smem_total = tp.smem_sort + pw * 8;
+    if ((size_t)tp.smem_total + 2048 > ix->max_smem) return PDXG_OK;
+    // replay: k1 = the L1 nprobe (the top-level search's k), per-warp shared memory
+    tp.ratios = ix->d_ratios;
+    tp.k1 = L.p.nprobe;
+    uint32_t maxn0 = 1;
+    for (uint32_t x : l0.n) maxn0 = std::max(maxn0, x);
+    uint32_t hcap = 1;
+    while (hcap < tp.k1) hcap <<= 1;
+    uint32_t scap = 1;
+    while (scap < std::max(maxn0, tp.k1)) scap <<= 1;
+    tp.r_dist_cap = (maxn0 + 31) / 32 * 32;
+    tp.r_sort_cap = scap;
+    tp.r_heap_cap = hcap;
+    tp.r_warp_bytes = (uint32_t)align_up((uint64_t)scap * 8 + (uint64_t)hcap * 8 + (uint64_t)tp.r_dist_cap * 8, 16);
+    if ((size_t)tp.r_warp_bytes * 8 + 1024 > ix->max_smem) return PDXG_OK;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * tp.k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    tp.l1_order = w.d_l1_order;
+    tp.l1_count = w.d_l1_count;
+    PDXG_CUDA(launch_top_level(tp, st));
+    L.p.q_order = w.d_l1_order;
+    L.p.q_order_count = w.d_l1_count;
+    L.p.q_order_stride = tp.k1;
+    return PDXG_OK;
+}
+
 // Core device-side search: queries/ids/dists/counts are device pointers.
 int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, uint32_t flags,
                        const uint32_t* d_order, uint32_t n_order, const uint32_t* d_sel,
@@ -641,6 +753,10 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     Launch L;
     rc = plan_search(ix, nq, k, n_order, any_filter, L);
     if (rc) return rc;
+    if (ix->tree && !any_filter && !d_order) {
+        rc = run_top_level(ix, qp, nq, L, st);
+        if (rc) return rc;
+    }
     L.p.queries = qp;
     L.p.order = d_order;
     L.p.sel_bits = d_sel;
@@ -652,8 +768,8 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     L.p.queue = ix->ws.d_queue;
     L.p.stats = nullptr;
     if (flags & PDXG_COLLECT_STATS) {
-        if (!ix->ws.d_stats) PDXG_CUDA(cudaMalloc(&ix->ws.d_stats, 9 * sizeof(unsigned long long)));
-        PDXG_CUDA(cudaMemsetAsync(ix->ws.d_stats, 0, 9 * sizeof(unsigned long long), st));
+        if (!ix->ws.d_stats) PDXG_CUDA(cudaMalloc(&ix->ws.d_stats, 12 * sizeof(unsigned long long)));
+        PDXG_CUDA(cudaMemsetAsync(ix->ws.d_stats, 0, 12 * sizeof(unsigned long long), st));
         L.p.stats = ix->ws.d_stats;
         ix->stats_stream = st;
     }
@@ -819,6 +935,13 @@ int pdxg_set_pruning_aggressiveness(pdxg_index* ix, float eps0) {
     return upload_ratios(ix);
 }
 
+int pdxg_set_top_level_mode(pdxg_index* ix, uint32_t mode) {
+    if (int rc = check_index(ix)) return rc;
+    if (mode > 2) return fail(PDXG_ERR_INVALID_ARGUMENT, "top-level mode must be 0, 1 or 2");
+    ix->top_mode = mode;
+    return PDXG_OK;
+}
+
 int pdxg_set_threads_per_query(pdxg_index* ix, uint32_t threads) {
     if (int rc = check_index(ix)) return rc;
     if (threads != 0 && threads != 128 && threads != 256 && threads != 512)
@@ -924,16 +1047,16 @@ int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, floa
     return PDXG_OK;
 }
 
-int pdxg_get_stats(pdxg_index* ix, uint64_t out[9]) {
+int pdxg_get_stats(pdxg_index* ix, uint64_t out[12]) {
     if (int rc = check_index(ix)) return rc;
     if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
     std::lock_guard<std::mutex> lock(ix->mu);
     if (!ix->ws.d_stats) return fail(PDXG_ERR_INVALID_ARGUMENT, "no search ran with PDXG_COLLECT_STATS");
     PDXG_CUDA(cudaSetDevice(ix->device));
     PDXG_CUDA(cudaStreamSynchronize(ix->stats_stream ? ix->stats_stream : ix->stream));
-    unsigned long long h[9];
+    unsigned long long h[12];
     PDXG_CUDA(cudaMemcpy(h, ix->ws.d_stats, sizeof(h), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < 9; ++i) out[i] = h[i];
+    for (int i = 0; i < 12; ++i) out[i] = h[i];
     return PDXG_OK;
 }
 

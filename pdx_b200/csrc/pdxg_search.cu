@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "pdxg_block.cuh"
 #include "pdxg_common.cuh"
 
 namespace pdxg {
@@ -45,189 +46,11 @@ struct Shared {
     uint64_t* sorth;    // heap region viewed as u64 [heap_cap]
 };
 
-struct Scalars {
-    uint32_t warp[32];
-    uint32_t hist[256];
-    uint32_t sc[4];
-    uint32_t hsize;
-    uint32_t top_slot;
-    float top;
-    uint32_t query;
-    uint32_t n_order;
-    unsigned long long bytes[6];  // algorithmic bytes of the current query by phase (stats only)
-    unsigned long long visits;
-    unsigned long long merged;
-};
 
-// Phases of the algorithmic-byte accounting (stats[3 + phase]).
-enum Phase { kTopLevel = 0, kStart = 1, kWarmup = 2, kSurvivorH = 3, kSurvivorV = 4, kProbe = 5 };
 
-__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
-__device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
-
-template <int T>
-__device__ __forceinline__ uint32_t block_sum(uint32_t x, Scalars& s) {
-    constexpr int NW = T / 32;
-    x = __reduce_add_sync(0xffffffffu, x);
-    if (lane_id() == 0) s.warp[warp_id()] = x;
-    __syncthreads();
-    uint32_t tot = 0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) tot += s.warp[w];
-    __syncthreads();
-    return tot;
-}
-
-// Order-preserving compaction of i in [0, n) with pred(i): out[rank] = val(i).
-// In-place use (out aliasing the array val() reads) is safe: every element of a chunk is
-// read before the chunk's writes, and writes never reach past the current chunk.
-template <int T, class Pred, class Val>
-__device__ uint32_t block_compact(uint32_t n, Pred pred, Val val, uint32_t* out, Scalars& s) {
-    constexpr int NW = T / 32;
-    const uint32_t lane = lane_id(), warp = warp_id();
-    uint32_t total = 0;
-    for (uint32_t c0 = 0; c0 < n; c0 += T) {
-        const uint32_t i = c0 + threadIdx.x;
-        const bool in = i < n;
-        const uint32_t v = in ? val(i) : 0u;
-        const bool p = in && pred(i, v);
-        const unsigned b = __ballot_sync(0xffffffffu, p);
-        if (lane == 0) s.warp[warp] = __popc(b);
-        __syncthreads();
-        uint32_t off = total, ctot = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const uint32_t c = s.warp[w];
-            off += (w < (int)warp) ? c : 0u;
-            ctot += c;
-        }
-        if (p) out[off + __popc(b & ((1u << lane) - 1u))] = v;
-        total += ctot;
-        __syncthreads();
-    }
-    return total;
-}
-
-// Exact selection: kth = the m-th smallest key (1 <= m <= n), less = #keys < kth.
-template <int T>
-__device__ void block_radix_select(const uint32_t* keys, uint32_t n, uint32_t m, Scalars& s,
-                                   uint32_t& kth, uint32_t& less) {
-    uint32_t prefix = 0, mask = 0, rem = m, acc_less = 0;
-    for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += T) s.hist[i] = 0;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += T) {
-            const uint32_t k = keys[i];
-            if ((k & mask) == prefix) atomicAdd(&s.hist[(k >> shift) & 255u], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const uint32_t lane = lane_id();
-            uint32_t loc[8], sum = 0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                loc[j] = s.hist[lane * 8 + j];
-                sum += loc[j];
-            }
-            uint32_t incl = sum;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= (uint32_t)off) incl += t;
-            }
-            const uint32_t excl = incl - sum;
-            const bool mine = excl < rem && rem <= incl;
-            const unsigned bm = __ballot_sync(0xffffffffu, mine);
-            if (lane == (uint32_t)(__ffs(bm) - 1)) {
-                uint32_t c = excl;
-                int b = 0;
-                for (; b < 7; ++b) {
-                    if (c + loc[b] >= rem) break;
-                    c += loc[b];
-                }
-                s.sc[0] = lane * 8 + b;
-                s.sc[1] = c;
-            }
-        }
-        __syncthreads();
-        const uint32_t bin = s.sc[0], cum = s.sc[1];
-        prefix |= bin << shift;
-        mask |= 0xFFu << shift;
-        rem -= cum;
-        acc_less += cum;
-        __syncthreads();
-    }
-    kth = prefix;
-    less = acc_less;
-}
-
-// Ascending bitonic sort of N (power of two) u64 keys in shared memory.
-template <int T>
-__device__ void block_bitonic_sort(uint64_t* a, uint32_t N) {
-    for (uint32_t size = 2; size <= N; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t i = threadIdx.x; i < (N >> 1); i += T) {
-                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
-                const uint32_t hi = lo + stride;
-                const bool asc = (lo & size) == 0;
-                const uint64_t x = a[lo], y = a[hi];
-                if ((x > y) == asc) {
-                    a[lo] = y;
-                    a[hi] = x;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-__device__ __forceinline__ uint32_t next_pow2(uint32_t x) {
-    return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
-}
 
 // ------------------------------------------------------------------------------------------
 // Distances.
-
-// avx2_computers.hpp:47-98 over one 64-dim row, 8 threads per row (sub = lane & 7): lane j
-// accumulates dims j, j+8, ..., j+56 with FMA; lanes 0 of each 8-group return the f32 result.
-__device__ __forceinline__ float horiz64_f32_group8(const float* q, const float* x, uint32_t sub,
-                                                    bool active) {
-    float acc = 0.0f;
-    if (active) {
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const float d = __fsub_rn(q[sub + 8 * t], __ldg(x + sub + 8 * t));
-            acc = __fmaf_rn(d, d, acc);
-        }
-    }
-    double s = (double)acc + (double)__shfl_down_sync(0xffffffffu, acc, 4, 8);
-    s = s + __shfl_down_sync(0xffffffffu, s, 2, 8);
-    s = s + __shfl_down_sync(0xffffffffu, s, 1, 8);
-    return (float)s;
-}
-
-// Full-length avx2 Horizontal(q, x, d) for centroid probing, 8 threads per vector.
-__device__ __forceinline__ float horiz_f32_group8(const float* q, const float* x, uint32_t d,
-                                                  uint32_t sub, bool active) {
-    float acc = 0.0f;
-    const uint32_t full = d & ~7u;
-    if (active) {
-        for (uint32_t i = 0; i < full; i += 8) {
-            const float t = __fsub_rn(q[i + sub], __ldg(x + i + sub));
-            acc = __fmaf_rn(t, t, acc);
-        }
-    }
-    double s = (double)acc + (double)__shfl_down_sync(0xffffffffu, acc, 4, 8);
-    s = s + __shfl_down_sync(0xffffffffu, s, 2, 8);
-    s = s + __shfl_down_sync(0xffffffffu, s, 1, 8);
-    if (active && sub == 0) {
-        for (uint32_t i = full; i < d; ++i) {
-            const float t = __fsub_rn(q[i], __ldg(x + i));
-            s += (double)__fmul_rn(t, t);
-        }
-    }
-    return (float)s;
-}
 
 __device__ __forceinline__ uint32_t sqdiff4(uint32_t a, uint32_t b, uint32_t acc) {
     const uint32_t d = __vabsdiffu4(a, b);
@@ -651,10 +474,14 @@ struct LevelOps {
             if (c.n == 0) continue;
             if (p.stats && threadIdx.x == 0) s.visits += 1;
             if (s.hsize < k) {
+                long long t0 = 0;
+                if (p.stats && threadIdx.x == 0) t0 = clock64();
                 if (filter >= 0)
                     filtered_start(c, k, passing);
                 else
                     start(c, k);
+                if (p.stats && threadIdx.x == 0 && !top_level)
+                    s.cycles[1] += (unsigned long long)(clock64() - t0);
                 continue;
             }
             prune_cluster(c, k, passing);
@@ -774,24 +601,33 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         if (q >= p.nq) break;
         if (threadIdx.x == 0) {
             for (int i = 0; i < 6; ++i) s.bytes[i] = 0;
+            for (int i = 0; i < 3; ++i) s.cycles[i] = 0;
             s.visits = 0;
             s.merged = 0;
         }
         const int filter = p.filter_of ? p.filter_of[q] : -1;
         prepare_query<T>(p, sh, q);
 
+        long long t_q0 = 0;
+        if (p.stats && threadIdx.x == 0) t_q0 = clock64();
         uint32_t nvisit;
         if (p.order) {
             // caller-provided access order (PDXearch::SetClusterAccessOrder, searcher.hpp:48-54)
             nvisit = p.nprobe < p.n_order ? p.nprobe : p.n_order;
             for (uint32_t i = threadIdx.x; i < nvisit; i += T) sh.order[i] = __ldg(p.order + i);
             __syncthreads();
+        } else if (p.is_tree && filter < 0 && p.q_order) {
+            // batched tree top level (pdxg_toplevel.cu) already produced this query's L1 order
+            nvisit = __ldg(p.q_order_count + q);
+            for (uint32_t i = threadIdx.x; i < nvisit; i += T)
+                sh.order[i] = __ldg(p.q_order + (size_t)q * p.q_order_stride + i);
+            __syncthreads();
         } else if (p.is_tree && filter < 0) {
             // PDXTreeIndex::Search (index.hpp:545-566): pruned F32 search over the meso
             // clusters with k = nprobe returns the L1 clusters to visit, nearest first.
             LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
-            top.probe(p.top_nprobe);
             const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
+            top.probe(p.top_nprobe);
             top.run(p.nprobe, nv0);
             const uint32_t cnt = top.sort_heap(p.nprobe);
             for (uint32_t i = threadIdx.x; i < cnt; i += T) sh.order[i] = (uint32_t)sh.sortw[i];
@@ -802,6 +638,11 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             nvisit = probe_ops.probe(p.nprobe);
         }
 
+        if (p.stats && threadIdx.x == 0) {
+            const long long now = clock64();
+            s.cycles[0] += (unsigned long long)(now - t_q0);
+            t_q0 = now;
+        }
         LevelOps<T, U8> ops(p, p.l1, sh, s, filter);
         ops.run(p.k, nvisit);
         const uint32_t cnt = ops.sort_heap(p.k);
@@ -820,6 +661,8 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         if (threadIdx.x == 0) {
             p.out_counts[q] = cnt;
             if (p.stats) {
+                s.cycles[2] += (unsigned long long)(clock64() - t_q0) - s.cycles[1];
+                for (int i = 0; i < 3; ++i) atomicAdd(p.stats + 9 + i, s.cycles[i]);
                 unsigned long long tot = 0;
                 for (int i = 0; i < 6; ++i) {
                     tot += s.bytes[i];

@@ -239,3 +239,55 @@ def test_filtered_edge_cases():
     a = ix.filtered_search(q[1], 10, all_rows)
     b = ix.search(q[1], 10)
     np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("itype", ["pdx_tree_f32", "pdx_tree_u8"])
+@pytest.mark.parametrize("d", [65, 130, 384])
+def test_tree_top_level_modes(port_cls, itype, d):
+    """The batched top level (probe + exact partials + replay) gives the same results as the
+    per-query top level and as the oracle."""
+    gm = GaussianMixture(d, 20, 0.5, seed=d + 3, unit_norm=True)
+    X = gm.sample(4000, 0)
+    Q = gm.sample(80, 1)
+    f = build_index(X, itype, num_clusters=40, num_meso_clusters=7, normalize=True, seed=3)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        port = port_cls(p)
+        ix = compiled.load_index(p)
+        R = ix.prepare_queries(Q)
+        for nprobe in (0, 3, 12, 39):
+            ix.set_nprobe(nprobe)
+            port.set_nprobe(nprobe)
+            res = {}
+            for mode in (1, 2):
+                ix.set_top_level_mode(mode)
+                res[mode] = ix.search_batch(R, 10, transformed=True)
+            for i in range(len(R)):
+                pi, pd = port.search(R[i], 10, transformed=True)
+                for mode in (1, 2):
+                    ids, ds, cnt = res[mode]
+                    assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd,
+                                ctx=f"{itype} d={d} nprobe={nprobe} mode={mode} q{i}")
+        port.close()
+
+
+def test_tree_top_level_batched_edge_sizes(port_cls):
+    for itype in ("pdx_tree_f32", "pdx_tree_u8"):
+        f, X = _manual_index(itype, 200, [0, 1, 31, 33, 0, 5, 64, 257, 2, 0, 90, 7])
+        Q = np.random.default_rng(5).standard_normal((40, 200)).astype(np.float32)
+        with tempfile.TemporaryDirectory() as td:
+            p = os.path.join(td, "ix.pdx")
+            f.save(p)
+            port = port_cls(p)
+            ix = compiled.load_index(p)
+            ix.set_top_level_mode(2)
+            R = ix.prepare_queries(Q)
+            for nprobe, k in ((0, 10), (2, 10), (5, 500)):
+                ix.set_nprobe(nprobe)
+                port.set_nprobe(nprobe)
+                ids, ds, cnt = ix.search_batch(R, k, transformed=True)
+                for i in range(len(R)):
+                    pi, pd = port.search(R[i], k, transformed=True)
+                    assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd, ctx=f"{itype} nprobe={nprobe} k={k} q{i}")
+            port.close()
