@@ -161,7 +161,7 @@ int pdxg_search_device_noalloc(pdxg_index* index, const float* queries, uint32_t
 uint64_t pdxg_noalloc_scratch_bytes(void);
 
 /* Engine tuning, tree indexes: how the top-level (meso-cluster) search runs. 0 = automatic
- * (batched for batches of 32+ queries), 1 = inside each query's search CTA, 2 = batched: a probe
+ * (currently the per-query form), 1 = inside each query's search CTA, 2 = batched: a probe
  * kernel and a partials kernel compute, for all queries at once, the exact values the
  * top-level decisions depend on, and each query replays PDXTreeIndex::Search's decisions
  * (index.hpp:545-566) on them. Results are identical in every mode. */

@@ -107,7 +107,7 @@ struct TopLevelParams {
     uint32_t k1;                          // L1 clusters to return per query (the L1 nprobe)
     uint32_t* l1_order;                   // [nq x k1]
     uint32_t* l1_count;                   // [nq]
-    uint32_t r_dist_cap, r_sort_cap, r_heap_cap, r_warp_bytes;
+    uint32_t r_dist_cap, r_sort_cap, r_heap_cap, r_warp_bytes, r_warps_per_block;
 };
 
 }  // namespace pdxg

@@ -287,7 +287,7 @@ __device__ __forceinline__ void warp_heap_top(const float* hd, uint32_t hsize, f
 __global__ void __launch_bounds__(256) top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t q = blockIdx.x * 8 + warp;
+    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + warp;
     if (q >= tp.nq) return;  // whole warp
     uint8_t* base = smem + (size_t)warp * tp.r_warp_bytes;
     uint64_t* sortbuf = reinterpret_cast<uint64_t*>(base);
@@ -445,10 +445,11 @@ cudaError_t launch_top_level(const TopLevelParams& tp, cudaStream_t st) {
     meso_partials_kernel<<<grid, 256, 0, st>>>(tp);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const size_t rsmem = (size_t)tp.r_warp_bytes * 8;
+    const uint32_t wpb = tp.r_warps_per_block;
+    const size_t rsmem = (size_t)tp.r_warp_bytes * wpb;
     e = cudaFuncSetAttribute(top_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem);
     if (e != cudaSuccess) return e;
-    top_replay_kernel<<<(tp.nq + 7) / 8, 256, rsmem, st>>>(tp);
+    top_replay_kernel<<<(tp.nq + wpb - 1) / wpb, 32 * wpb, rsmem, st>>>(tp);
     return cudaGetLastError();
 }
 
