@@ -196,6 +196,8 @@ def main():
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--threads", type=int, default=0, help="threads per query CTA (0 = auto)")
+    ap.add_argument("--top-mode", type=int, default=None,
+                    help="tree top level: 0 auto, 1 per query, 2 batched warp-per-query kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
     ap.add_argument("--sweep", action="store_true",
@@ -239,6 +241,8 @@ def main():
     ix.set_nprobe(cfg["nprobe"])
     if args.threads:
         ix.set_threads_per_query(args.threads)
+    if args.top_mode is not None:
+        ix.set_top_level_mode(args.top_mode)
     nq, k, d = cfg["nq"], cfg["k"], cfg["d"]
     Qh = gm.sample(nq, 1 + rank)  # rank-specific batch; the first GT_QUERIES match the GT
     # a dedicated stream: the events below and the engine's launches must share it (handle 0,

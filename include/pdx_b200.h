@@ -160,11 +160,11 @@ int pdxg_search_device_noalloc(pdxg_index* index, const float* queries, uint32_t
 /* PDXG_NOALLOC_SCRATCH_BYTES as built into the library. */
 uint64_t pdxg_noalloc_scratch_bytes(void);
 
-/* Engine tuning, tree indexes: how the top-level (meso-cluster) search runs. 0 = automatic
- * (currently the per-query form), 1 = inside each query's search CTA, 2 = batched: a probe
- * kernel and a partials kernel compute, for all queries at once, the exact values the
- * top-level decisions depend on, and each query replays PDXTreeIndex::Search's decisions
- * (index.hpp:545-566) on them. Results are identical in every mode. */
+/* Engine tuning, tree indexes: how the top-level (meso-cluster) search of
+ * PDXTreeIndex::Search (index.hpp:545-566) runs. 0 = automatic (its own launch when it fits),
+ * 1 = inside each query's search CTA, 2 = its own launch of small per-query CTAs that write the
+ * L1 visit orders the search kernel then reads (fails with PDXG_ERR_CAPACITY if it cannot run).
+ * Results are identical in every mode. */
 int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
 
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */

@@ -299,7 +299,7 @@ class PDXIndex:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))
 
     def set_top_level_mode(self, mode: int) -> None:
-        """Tree indexes: 0 automatic, 1 per-query top-level search, 2 batched two-phase."""
+        """Tree indexes: 0 automatic, 1 top level inside each query's CTA, 2 own launch."""
         _check(library().pdxg_set_top_level_mode(self._handle().ptr, int(mode)))
 
     def set_threads_per_query(self, threads: int) -> None:

@@ -84,30 +84,4 @@ struct SearchParams {
     uint32_t order_cap;          // entries of the cluster order list
 };
 
-// The batched top-level stage (pdxg_toplevel.cu).
-struct TopLevelParams {
-    const uint8_t* arena;
-    DevLevel l0;
-    const float* queries;                 // prepared queries [nq x d]
-    uint32_t nq;
-    uint32_t top;                         // meso clusters probed per query
-    uint32_t nvals;                       // values per (query, vector): n_ckpt + l0.n_hblocks
-    uint32_t n_ckpt;
-    uint32_t ckpt[kNumFetchSizes + 1];    // cumulative warmup boundaries, capped at d_v
-    unsigned long long per_query_floats;  // partial-value budget of one query
-    uint32_t* order;                      // [nq x top] meso ids, nearest first
-    unsigned long long* offsets;          // [nq x top] float offsets into vals
-    uint32_t* lists;                      // [n0 x nq] entries q * top + rank
-    uint32_t* list_count;                 // [n0]
-    float* vals;
-    uint32_t n0_cap;                      // dist/pos entries in the probe's shared memory
-    uint32_t smem_dist, smem_sort, smem_total;
-    // replay (warp per query)
-    const float* ratios;
-    uint32_t k1;                          // L1 clusters to return per query (the L1 nprobe)
-    uint32_t* l1_order;                   // [nq x k1]
-    uint32_t* l1_count;                   // [nq]
-    uint32_t r_dist_cap, r_sort_cap, r_heap_cap, r_warp_bytes, r_warps_per_block;
-};
-
 }  // namespace pdxg

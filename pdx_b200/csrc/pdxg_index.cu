@@ -23,7 +23,8 @@ cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid,
 int search_occupancy(bool u8, int threads, size_t smem);
 cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, const float* rotation,
                                    bool normalize, float* norms_ws, float* out, cudaStream_t st);
-cudaError_t launch_top_level(const TopLevelParams& tp, cudaStream_t st);
+cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st);
+int top_level_occupancy(size_t smem);
 }  // namespace pdxg
 
 using namespace pdxg;
@@ -288,7 +289,7 @@ struct pdxg_index {
     float eps0 = 1.5f;
     uint32_t nprobe = 0;
     uint32_t threads = 0;
-    uint32_t top_mode = 0;  // tree top level: 0 auto, 1 fused per query, 2 batched two-phase
+    uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch
     int num_sms = 0;
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
@@ -642,102 +643,59 @@ int ensure_ws(pdxg_index* ix, uint32_t nq, uint32_t k) {
         if ((rc = dev_grow(w.d_dists, cap, (uint64_t)w.q_cap * k))) return rc;
         w.k_cap = k;
     }
-    if (!w.d_queue) PDXG_CUDA(cudaMalloc(&w.d_queue, sizeof(uint32_t)));
+    if (!w.d_queue) PDXG_CUDA(cudaMalloc(&w.d_queue, 4 * sizeof(uint32_t)));  // search, -, top
     return PDXG_OK;
 }
 
-// Warmup checkpoints: cumulative DIMENSIONS_FETCHING_SIZES capped at d_v (common.hpp:47-49).
-uint32_t warmup_checkpoints(uint32_t dv, uint32_t* out) {
-    static const uint32_t sizes[kNumFetchSizes] = {16,  16,  32,  32,  32,   32,   64,
-                                                   64,  64,  64,  128, 128,  128,  128,
-                                                   256, 256, 512, 1024, 2048, 16384};
-    uint32_t n = 0, cur = 0, step = 0;
-    while (cur < dv && n < (uint32_t)kNumFetchSizes) {
-        uint32_t last = cur + sizes[step < (uint32_t)kNumFetchSizes ? step : kNumFetchSizes - 1];
-        if (last > dv) last = dv;
-        out[n++] = last;
-        cur = last;
-        ++step;
-    }
-    return n;
-}
-
-// Batched tree top level (pdxg_toplevel.cu): fills L.p.top_* on success; leaves them NULL (the
-// search kernel then runs the fused per-query top level) when the mode or the batch says so.
+// Tree top level as its own launch of small CTAs (top_level_kernel): on success the search
+// kernel reads each query's L1 order from L.p.q_order; in the per-query mode the search kernel
+// runs the top level itself.
 int run_top_level(pdxg_index* ix, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
-    // automatic mode keeps the fused per-query top level: measured faster on B200 for the
-    // 1M x 1024 two-level workload (the batched form is bit-identical and selectable)
-    if (ix->top_mode != 2) return PDXG_OK;
-    // mode 2 (forced) reports why the batched form cannot run; mode 0 falls back silently
-    auto unavailable = [&](const char* why) {
-        return ix->top_mode == 2 ? fail(PDXG_ERR_CAPACITY, why) : PDXG_OK;
-    };
-    const HostLevel& l0 = ix->l0;
-    const uint32_t n0 = (uint32_t)l0.fc.size();
-    const uint32_t top = std::min(L.p.top_nprobe, n0);
-    if (top == 0) return PDXG_OK;
-    TopLevelParams tp{};
-    tp.arena = ix->arena;
-    tp.l0 = L.p.l0;
+    if (ix->top_mode == 1) return PDXG_OK;
+    SearchParams tp = L.p;
     tp.queries = qp;
-    tp.nq = nq;
-    tp.top = top;
-    tp.n_ckpt = warmup_checkpoints(ix->dv, tp.ckpt);
-    tp.ckpt[tp.n_ckpt] = 0xFFFFFFFFu;
-    tp.nvals = tp.n_ckpt + l0.n_hblocks;
-    std::vector<uint32_t> sizes(l0.n.begin(), l0.n.end());
-    std::sort(sizes.begin(), sizes.end(), std::greater<uint32_t>());
-    uint64_t budget = 0;
-    for (uint32_t i = 0; i < top; ++i) budget += sizes[i];
-    tp.per_query_floats = budget * tp.nvals;
-    const uint64_t vals = (uint64_t)nq * tp.per_query_floats;
-    if (vals * 4 > (8ull << 30)) return unavailable("batched top level needs more than 8 GB of workspace");
+    const uint32_t k1 = L.p.nprobe;
+    const uint32_t top = L.p.top_nprobe;
+    // shared memory of one top-level CTA: query, work (meso clusters / probe), heap, order
+    const uint32_t heap_cap = next_pow2(std::max({k1, top, 1u}));
+    uint32_t work = std::max({tp.l0.max_n, tp.l0.nclusters, heap_cap, 32u});
+    const uint32_t work_cap = (work + 31) / 32 * 32;
+    uint32_t off = 0;
+    tp.smem_qf = 0;
+    off += (uint32_t)align_up((uint64_t)ix->d * 4, 16);
+    tp.smem_qw = off;
+    tp.smem_work = off;
+    off += work_cap * 8;
+    tp.smem_heap = off;
+    off += heap_cap * 8;
+    tp.smem_order = off;
+    off += (uint32_t)align_up((uint64_t)std::max(top, 1u) * 4, 16);
+    tp.smem_total = off;
+    tp.work_cap = work_cap;
+    tp.heap_cap = heap_cap;
+    tp.order_cap = top;
+    if ((size_t)off + 2048 > ix->max_smem) {
+        if (ix->top_mode == 2) return fail(PDXG_ERR_CAPACITY, "top-level kernel does not fit in shared memory");
+        return PDXG_OK;
+    }
     Workspace& w = ix->ws;
     int rc;
-    if ((rc = dev_grow(w.d_top_order, w.top_order_cap, (uint64_t)nq * top))) return rc;
-    if ((rc = dev_grow(w.d_top_off, w.top_off_cap, (uint64_t)nq * top))) return rc;
-    if ((rc = dev_grow(w.d_top_lists, w.top_lists_cap, (uint64_t)n0 * nq))) return rc;
-    if ((rc = dev_grow(w.d_top_count, w.top_count_cap, n0))) return rc;
-    if ((rc = dev_grow(w.d_top_vals, w.top_vals_cap, std::max<uint64_t>(vals, 1)))) return rc;
-    tp.order = w.d_top_order;
-    tp.offsets = w.d_top_off;
-    tp.lists = w.d_top_lists;
-    tp.list_count = w.d_top_count;
-    tp.vals = w.d_top_vals;
-    tp.n0_cap = (n0 + 31) / 32 * 32;
-    uint32_t pw = 1;
-    while (pw < top) pw <<= 1;
-    tp.smem_dist = (uint32_t)align_up((uint64_t)ix->d * 4, 16);
-    tp.smem_sort = tp.smem_dist + tp.n0_cap * 8;
-    tp.smem_total = tp.smem_sort + pw * 8;
-    if ((size_t)tp.smem_total + 2048 > ix->max_smem)
-        return unavailable("meso probe does not fit in shared memory");
-    // replay: k1 = the L1 nprobe (the top-level search's k), per-warp shared memory
-    tp.ratios = ix->d_ratios;
-    tp.k1 = L.p.nprobe;
-    uint32_t maxn0 = 1;
-    for (uint32_t x : l0.n) maxn0 = std::max(maxn0, x);
-    uint32_t hcap = 1;
-    while (hcap < tp.k1) hcap <<= 1;
-    uint32_t scap = 1;
-    while (scap < std::max(maxn0, tp.k1)) scap <<= 1;
-    tp.r_dist_cap = (maxn0 + 31) / 32 * 32;
-    tp.r_sort_cap = scap;
-    tp.r_heap_cap = hcap;
-    tp.r_warp_bytes = (uint32_t)align_up((uint64_t)scap * 8 + (uint64_t)hcap * 8 + (uint64_t)tp.r_dist_cap * 8, 16);
-    tp.r_warps_per_block = (uint32_t)std::min<size_t>(8, (ix->max_smem - 1024) / tp.r_warp_bytes);
-    if (tp.r_warps_per_block == 0)
-        return unavailable("largest meso cluster too large for the replay's shared memory");
-    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * tp.k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
     if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
-    tp.l1_order = w.d_l1_order;
-    tp.l1_count = w.d_l1_count;
-    PDXG_CUDA(launch_top_level(tp, st));
+    tp.q_order = w.d_l1_order;
+    tp.q_order_count = w.d_l1_count;
+    tp.q_order_stride = k1;
+    tp.queue = w.d_queue + 2;
+    PDXG_CUDA(cudaMemsetAsync(tp.queue, 0, sizeof(uint32_t), st));
+    const int occ = top_level_occupancy(off);
+    if (occ <= 0) return fail(PDXG_ERR_CAPACITY, "top-level kernel cannot be resident");
+    const int grid = (int)std::min<uint64_t>(nq, (uint64_t)occ * ix->num_sms);
+    PDXG_CUDA(launch_top_level(tp, grid, st));
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
-    L.p.q_order_stride = tp.k1;
+    L.p.q_order_stride = k1;
     return PDXG_OK;
 }
 
@@ -762,10 +720,6 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     Launch L;
     rc = plan_search(ix, nq, k, n_order, any_filter, L);
     if (rc) return rc;
-    if (ix->tree && !any_filter && !d_order) {
-        rc = run_top_level(ix, qp, nq, L, st);
-        if (rc) return rc;
-    }
     L.p.queries = qp;
     L.p.order = d_order;
     L.p.sel_bits = d_sel;
@@ -781,6 +735,10 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
         PDXG_CUDA(cudaMemsetAsync(ix->ws.d_stats, 0, 12 * sizeof(unsigned long long), st));
         L.p.stats = ix->ws.d_stats;
         ix->stats_stream = st;
+    }
+    if (ix->tree && !any_filter && !d_order) {
+        rc = run_top_level(ix, qp, nq, L, st);
+        if (rc) return rc;
     }
     PDXG_CUDA(cudaMemsetAsync(ix->ws.d_queue, 0, sizeof(uint32_t), st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));

@@ -115,55 +115,79 @@ struct LevelOps {
     // Vertical dims [d0, d1) for all vectors; returns #vectors with dist >= thr (counted only
     // when count is set). For U8, d0 is a multiple of 4; a trailing partial group is reached
     // only with d1 == dv and its padding bytes are zero in both query and data.
+    // Each thread keeps kVPT vectors (v, v + T, ...) and issues a whole batch of rows for all of
+    // them before consuming any, so one step costs one memory round trip, not one per vector.
+    static constexpr int kVPT = 4;
     __device__ uint32_t vertical_all(const DevCluster& c, uint32_t d0, uint32_t d1, bool count,
                                      uint32_t thr) {
         const uint32_t* base = vert(c);
         const uint32_t n = c.n, np = c.n_pad;
         uint32_t pruned = 0;
-        if constexpr (U8) {
-            const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
-            for (uint32_t v = threadIdx.x; v < n; v += T) {
-                uint32_t acc = sh.dist[v];
-                uint32_t g = g0;
-                for (; g + 4 <= g1; g += 4) {
-                    const uint32_t x0 = __ldg(base + (size_t)g * np + v);
-                    const uint32_t x1 = __ldg(base + (size_t)(g + 1) * np + v);
-                    const uint32_t x2 = __ldg(base + (size_t)(g + 2) * np + v);
-                    const uint32_t x3 = __ldg(base + (size_t)(g + 3) * np + v);
-                    acc = sqdiff4(sh.qw[g], x0, acc);
-                    acc = sqdiff4(sh.qw[g + 1], x1, acc);
-                    acc = sqdiff4(sh.qw[g + 2], x2, acc);
-                    acc = sqdiff4(sh.qw[g + 3], x3, acc);
+        for (uint32_t v0 = threadIdx.x; v0 < n; v0 += T * kVPT) {
+            bool act[kVPT];
+#pragma unroll
+            for (int k = 0; k < kVPT; ++k) act[k] = v0 + k * T < n;
+            if constexpr (U8) {
+                constexpr int GB = 8;  // groups per batch
+                const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
+                uint32_t acc[kVPT];
+#pragma unroll
+                for (int k = 0; k < kVPT; ++k) acc[k] = act[k] ? sh.dist[v0 + k * T] : 0u;
+                for (uint32_t g = g0; g < g1; g += GB) {
+                    uint32_t x[kVPT][GB];
+#pragma unroll
+                    for (int j = 0; j < GB; ++j)
+#pragma unroll
+                        for (int k = 0; k < kVPT; ++k)
+                            x[k][j] = (act[k] && g + j < g1) ? __ldg(base + (size_t)(g + j) * np + v0 + k * T) : 0u;
+#pragma unroll
+                    for (int j = 0; j < GB; ++j) {
+                        if (g + j < g1) {
+                            const uint32_t qv = sh.qw[g + j];
+#pragma unroll
+                            for (int k = 0; k < kVPT; ++k) acc[k] = sqdiff4(qv, x[k][j], acc[k]);
+                        }
+                    }
                 }
-                for (; g < g1; ++g) acc = sqdiff4(sh.qw[g], __ldg(base + (size_t)g * np + v), acc);
-                sh.dist[v] = acc;
-                pruned += (count && acc >= thr) ? 1u : 0u;
-            }
-        } else {
-            const float* fb = reinterpret_cast<const float*>(base);
-            for (uint32_t v = threadIdx.x; v < n; v += T) {
-                float acc = __uint_as_float(sh.dist[v]);
-                uint32_t j = d0;
-                for (; j + 4 <= d1; j += 4) {
-                    const float x0 = __ldg(fb + (size_t)j * np + v);
-                    const float x1 = __ldg(fb + (size_t)(j + 1) * np + v);
-                    const float x2 = __ldg(fb + (size_t)(j + 2) * np + v);
-                    const float x3 = __ldg(fb + (size_t)(j + 3) * np + v);
-                    float t = __fsub_rn(sh.qf[j], x0);
-                    acc = __fmaf_rn(t, t, acc);
-                    t = __fsub_rn(sh.qf[j + 1], x1);
-                    acc = __fmaf_rn(t, t, acc);
-                    t = __fsub_rn(sh.qf[j + 2], x2);
-                    acc = __fmaf_rn(t, t, acc);
-                    t = __fsub_rn(sh.qf[j + 3], x3);
-                    acc = __fmaf_rn(t, t, acc);
+#pragma unroll
+                for (int k = 0; k < kVPT; ++k) {
+                    if (act[k]) {
+                        sh.dist[v0 + k * T] = acc[k];
+                        pruned += (count && acc[k] >= thr) ? 1u : 0u;
+                    }
                 }
-                for (; j < d1; ++j) {
-                    const float t = __fsub_rn(sh.qf[j], __ldg(fb + (size_t)j * np + v));
-                    acc = __fmaf_rn(t, t, acc);
+            } else {
+                constexpr int DB = 8;  // dims per batch
+                const float* fb = reinterpret_cast<const float*>(base);
+                float acc[kVPT];
+#pragma unroll
+                for (int k = 0; k < kVPT; ++k) acc[k] = act[k] ? __uint_as_float(sh.dist[v0 + k * T]) : 0.0f;
+                for (uint32_t j = d0; j < d1; j += DB) {
+                    float x[kVPT][DB];
+#pragma unroll
+                    for (int t = 0; t < DB; ++t)
+#pragma unroll
+                        for (int k = 0; k < kVPT; ++k)
+                            x[k][t] = (act[k] && j + t < d1) ? __ldg(fb + (size_t)(j + t) * np + v0 + k * T) : 0.0f;
+#pragma unroll
+                    for (int t = 0; t < DB; ++t) {
+                        if (j + t < d1) {
+                            const float qv = sh.qf[j + t];
+#pragma unroll
+                            for (int k = 0; k < kVPT; ++k) {
+                                const float dd = __fsub_rn(qv, x[k][t]);
+                                acc[k] = __fmaf_rn(dd, dd, acc[k]);
+                            }
+                        }
+                    }
                 }
-                sh.dist[v] = __float_as_uint(acc);
-                pruned += (count && acc >= __uint_as_float(thr)) ? 1u : 0u;
+#pragma unroll
+                for (int k = 0; k < kVPT; ++k) {
+                    if (act[k]) {
+                        sh.dist[v0 + k * T] = __float_as_uint(acc[k]);
+                        pruned += (count && acc[k] >= __uint_as_float(thr)) ? 1u : 0u;
+                    }
+                }
             }
         }
         return count ? block_sum<T>(pruned, s) : 0u;
@@ -198,44 +222,79 @@ struct LevelOps {
     }
 
     // Adds horizontal block b to the distances of positions[0, npos) (all vectors when
-    // all_vectors is set, npos = n).
+    // all_vectors is set, npos = n). Several rows per thread group are in flight at once.
     __device__ void horizontal(const DevCluster& c, uint32_t b, uint32_t npos, bool all_vectors) {
         const uint32_t np = c.n_pad;
         const uint32_t lane = lane_id();
         if constexpr (U8) {
+            constexpr int RPG = 4;  // rows per 4-thread group per pass
             const uint8_t* hb = p.arena + c.hor_off + (size_t)b * np * kHDim;
             const uint32_t* qh = sh.qw + lv.qw_hoff + b * 16;
             const uint32_t sub = lane & 3;
-            const uint32_t per_pass = T / 4;
+            const uint32_t groups = T / 4;
             const uint4 q4 = *reinterpret_cast<const uint4*>(qh + sub * 4);
-            for (uint32_t base = 0; base < npos; base += per_pass) {
-                const uint32_t i = base + (threadIdx.x >> 2);
-                const bool active = i < npos;
-                const uint32_t v = active ? (all_vectors ? i : sh.pos[i]) : 0u;
-                uint32_t acc = 0;
-                if (active) {
-                    const uint4 x = __ldg(reinterpret_cast<const uint4*>(hb + (size_t)v * kHDim) + sub);
-                    acc = sqdiff4(q4.x, x.x, acc);
-                    acc = sqdiff4(q4.y, x.y, acc);
-                    acc = sqdiff4(q4.z, x.z, acc);
-                    acc = sqdiff4(q4.w, x.w, acc);
+            for (uint32_t base = 0; base < npos; base += groups * RPG) {
+                uint32_t v[RPG];
+                bool active[RPG];
+                uint4 x[RPG];
+#pragma unroll
+                for (int r = 0; r < RPG; ++r) {
+                    const uint32_t i = base + r * groups + (threadIdx.x >> 2);
+                    active[r] = i < npos;
+                    v[r] = active[r] ? (all_vectors ? i : sh.pos[i]) : 0u;
                 }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                if (active && sub == 0) sh.dist[v] += acc;
+#pragma unroll
+                for (int r = 0; r < RPG; ++r)
+                    x[r] = active[r] ? __ldg(reinterpret_cast<const uint4*>(hb + (size_t)v[r] * kHDim) + sub)
+                                     : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+                for (int r = 0; r < RPG; ++r) {
+                    uint32_t acc = 0;
+                    acc = sqdiff4(q4.x, x[r].x, acc);
+                    acc = sqdiff4(q4.y, x[r].y, acc);
+                    acc = sqdiff4(q4.z, x[r].z, acc);
+                    acc = sqdiff4(q4.w, x[r].w, acc);
+                    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                    if (active[r] && sub == 0) sh.dist[v[r]] += acc;
+                }
             }
         } else {
+            constexpr int RPG = 2;  // rows per 8-thread group per pass
             const float* hb = reinterpret_cast<const float*>(p.arena + c.hor_off) + (size_t)b * np * kHDim;
             const float* qh = sh.qf + lv.dv + b * kHDim;
             const uint32_t sub = lane & 7;
-            const uint32_t per_pass = T / 8;
-            for (uint32_t base = 0; base < npos; base += per_pass) {
-                const uint32_t i = base + (threadIdx.x >> 3);
-                const bool active = i < npos;
-                const uint32_t v = active ? (all_vectors ? i : sh.pos[i]) : 0u;
-                const float h = horiz64_f32_group8(qh, hb + (size_t)v * kHDim, sub, active);
-                if (active && sub == 0)
-                    sh.dist[v] = __float_as_uint(__fadd_rn(__uint_as_float(sh.dist[v]), h));
+            const uint32_t groups = T / 8;
+            for (uint32_t base = 0; base < npos; base += groups * RPG) {
+                uint32_t v[RPG];
+                bool active[RPG];
+                float x[RPG][8];
+#pragma unroll
+                for (int r = 0; r < RPG; ++r) {
+                    const uint32_t i = base + r * groups + (threadIdx.x >> 3);
+                    active[r] = i < npos;
+                    v[r] = active[r] ? (all_vectors ? i : sh.pos[i]) : 0u;
+                }
+#pragma unroll
+                for (int r = 0; r < RPG; ++r)
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        x[r][t] = active[r] ? __ldg(hb + (size_t)v[r] * kHDim + sub + 8 * t) : 0.0f;
+#pragma unroll
+                for (int r = 0; r < RPG; ++r) {
+                    // avx2_computers.hpp:47-98: lane sub accumulates dims sub, sub+8, ... with FMA
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const float dd = __fsub_rn(qh[sub + 8 * t], x[r][t]);
+                        acc = __fmaf_rn(dd, dd, acc);
+                    }
+                    double sm = (double)acc + (double)__shfl_down_sync(0xffffffffu, acc, 4, 8);
+                    sm = sm + __shfl_down_sync(0xffffffffu, sm, 2, 8);
+                    sm = sm + __shfl_down_sync(0xffffffffu, sm, 1, 8);
+                    if (active[r] && sub == 0)
+                        sh.dist[v[r]] = __float_as_uint(__fadd_rn(__uint_as_float(sh.dist[v[r]]), (float)sm));
+                }
             }
         }
         __syncthreads();
@@ -675,6 +734,76 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         }
         __syncthreads();
     }
+}
+
+// ------------------------------------------------------------------------------------------
+// Tree top level as its own launch (PDXTreeIndex::Search, index.hpp:545-566): small CTAs, one
+// per query, run the same per-query top-level search as search_kernel's tree branch -- meso
+// probe, pruned F32 search over the meso clusters with k = L1 nprobe -- and write the sorted
+// L1 order. Meso clusters are small, so 64 threads keep busy and many more queries are in
+// flight than with the L1 search's 256-thread CTAs. search_kernel then reads p.q_order.
+template <int T>
+__global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ SearchParams p) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ Scalars s;
+    Shared sh;
+    sh.qf = reinterpret_cast<float*>(smem + p.smem_qf);
+    sh.qw = nullptr;
+    sh.dist = reinterpret_cast<uint32_t*>(smem + p.smem_work);
+    sh.pos = sh.dist + p.work_cap;
+    sh.sortw = reinterpret_cast<uint64_t*>(smem + p.smem_work);
+    sh.hd = reinterpret_cast<float*>(smem + p.smem_heap);
+    sh.hid = reinterpret_cast<uint32_t*>(smem + p.smem_heap) + p.heap_cap;
+    sh.sorth = reinterpret_cast<uint64_t*>(smem + p.smem_heap);
+    sh.order = reinterpret_cast<uint32_t*>(smem + p.smem_order);
+    uint32_t* out_order = const_cast<uint32_t*>(p.q_order);
+    uint32_t* out_count = const_cast<uint32_t*>(p.q_order_count);
+    for (;;) {
+        if (threadIdx.x == 0) s.query = atomicAdd(p.queue, 1u);
+        __syncthreads();
+        const uint32_t q = s.query;
+        __syncthreads();
+        if (q >= p.nq) break;
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 6; ++i) s.bytes[i] = 0;
+            s.visits = 0;
+            s.merged = 0;
+        }
+        const float* src = p.queries + (size_t)q * p.l0.d;
+        for (uint32_t i = threadIdx.x; i < p.l0.d; i += T) sh.qf[i] = __ldg(src + i);
+        __syncthreads();
+        LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
+        const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
+        top.probe(p.top_nprobe);
+        top.run(p.nprobe, nv0);
+        const uint32_t cnt = top.sort_heap(p.nprobe);
+        for (uint32_t i = threadIdx.x; i < cnt; i += T)
+            out_order[(size_t)q * p.q_order_stride + i] = (uint32_t)sh.sortw[i];
+        if (threadIdx.x == 0) {
+            out_count[q] = cnt;
+            if (p.stats) {
+                atomicAdd(p.stats + 3, s.bytes[kTopLevel]);
+                atomicAdd(p.stats, s.bytes[kTopLevel]);
+                atomicAdd(p.stats + 1, s.visits);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st) {
+    auto kern = top_level_kernel<64>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_total);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, 64, p.smem_total, st>>>(p);
+    return cudaGetLastError();
+}
+
+int top_level_occupancy(size_t smem) {
+    int blocks = 0;
+    cudaFuncSetAttribute(top_level_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, top_level_kernel<64>, 64, smem);
+    return blocks;
 }
 
 // ------------------------------------------------------------------------------------------
