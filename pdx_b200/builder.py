@@ -93,8 +93,15 @@ def _assign_numpy(x: np.ndarray, c: np.ndarray) -> np.ndarray:
     return out
 
 
-def kmeans(x: np.ndarray, k: int, iters: int = 10, seed: int = 42, device: Optional[str] = None):
-    """Lloyd k-means. Returns (centroids f32 [k, d], assignment int64 [n])."""
+def kmeans(x: np.ndarray, k: int, iters: int = 10, seed: int = 42, device: Optional[str] = None,
+           angular: bool = False):
+    """Lloyd k-means. Returns (centroids f32 [k, d], assignment int64 [n]).
+
+    angular: spherical k-means (unit-norm centroids, nearest = largest inner product), what the
+    reference's SuperKMeans does for normalized data (clustering.hpp:55-56). Without it, plain
+    L2 Lloyd on unit vectors lets the smallest-norm centroid absorb most points. Empty clusters
+    are re-seeded from random points.
+    """
     n, d = x.shape
     rng = np.random.default_rng([seed, 104729])
     init = rng.choice(n, size=k, replace=False) if k <= n else rng.integers(0, n, k)
@@ -102,25 +109,40 @@ def kmeans(x: np.ndarray, k: int, iters: int = 10, seed: int = 42, device: Optio
         import torch
         xt = torch.from_numpy(np.ascontiguousarray(x)).to(device)
         ct = xt[torch.from_numpy(init).to(device)].clone()
+        gen = torch.Generator(device="cpu").manual_seed(int(seed) * 7 + 3)
+
+        def norm_rows(c):
+            return c / c.norm(dim=1, keepdim=True).clamp(min=1e-30)
+
+        if angular:
+            ct = norm_rows(ct)
         step = max(1, (1 << 28) // max(1, k))
         for it in range(iters + 1):
             cn = (ct * ct).sum(1)
             assign = torch.empty(n, dtype=torch.int64, device=device)
-            for s in range(0, n, step):
-                xs = xt[s:s + step]
-                assign[s:s + step] = torch.argmin(cn[None, :] - 2.0 * (xs @ ct.T), dim=1)
+            for s0 in range(0, n, step):
+                xs = xt[s0:s0 + step]
+                assign[s0:s0 + step] = torch.argmin(cn[None, :] - 2.0 * (xs @ ct.T), dim=1)
             if it == iters:
                 break
             sums = torch.zeros_like(ct).index_add_(0, assign, xt)
             cnt = torch.bincount(assign, minlength=k).to(ct.dtype)
             empty = cnt == 0
-            ct = torch.where(empty[:, None], ct, sums / cnt.clamp(min=1)[:, None])
-        # final centroids are the means of the final assignment
-        sums = torch.zeros_like(ct).index_add_(0, assign, xt)
-        cnt = torch.bincount(assign, minlength=k).to(ct.dtype)
-        ct = torch.where((cnt == 0)[:, None], ct, sums / cnt.clamp(min=1)[:, None])
+            new_c = sums / cnt.clamp(min=1)[:, None]
+            if bool(empty.any()):
+                ridx = torch.randint(0, n, (int(empty.sum()),), generator=gen).to(device)
+                new_c[empty] = xt[ridx]
+            ct = norm_rows(new_c) if angular else new_c
         return ct.float().cpu().numpy(), assign.cpu().numpy()
     c = x[init].astype(np.float32).copy()
+
+    def norm_np(c):
+        nrm = np.linalg.norm(c, axis=1, keepdims=True)
+        nrm[nrm == 0] = 1.0
+        return (c / nrm).astype(np.float32)
+
+    if angular:
+        c = norm_np(c)
     for it in range(iters + 1):
         assign = _assign_numpy(x, c)
         if it == iters:
@@ -130,11 +152,10 @@ def kmeans(x: np.ndarray, k: int, iters: int = 10, seed: int = 42, device: Optio
         np.add.at(sums, assign, x)
         nz = cnt > 0
         c[nz] = (sums[nz] / cnt[nz, None]).astype(np.float32)
-    cnt = np.bincount(assign, minlength=k)
-    sums = np.zeros_like(c, dtype=np.float64)
-    np.add.at(sums, assign, x)
-    nz = cnt > 0
-    c[nz] = (sums[nz] / cnt[nz, None]).astype(np.float32)
+        if (~nz).any():
+            c[~nz] = x[rng.integers(0, n, int((~nz).sum()))]
+        if angular:
+            c = norm_np(c)
     return c, assign
 
 
@@ -174,7 +195,7 @@ def build_index(data: np.ndarray, index_type: str = "pdx_f32", num_clusters: int
     is_u8 = itype in (1, 3)
     if is_u8:
         base, scale = quantization_params(rot)
-    cents, assign = kmeans(rot, num_clusters, kmeans_iters, seed, device)
+    cents, assign = kmeans(rot, num_clusters, kmeans_iters, seed, device, angular=normalize)
     stored = _quantize(rot, base, scale, device) if is_u8 else rot
     row_ids = np.arange(n, dtype=np.uint32)
     embs, ids = _split_by_assignment(stored, row_ids, assign, num_clusters)
@@ -184,7 +205,7 @@ def build_index(data: np.ndarray, index_type: str = "pdx_f32", num_clusters: int
         n0 = num_meso_clusters or int(math.sqrt(num_clusters))
         if n0 >= num_clusters:
             raise ValueError("num_meso_clusters must be smaller than num_clusters")
-        c0, a0 = kmeans(cents, n0, 10, seed, None)
+        c0, a0 = kmeans(cents, n0, 10, seed, None, angular=normalize)
         e0, i0 = _split_by_assignment(cents, np.arange(num_clusters, dtype=np.uint32), a0, n0)
         l0 = Level(e0, i0, c0)
     return IndexFile(itype, rotation, d, l1, l0, bool(normalize), float(base), float(scale))
