@@ -202,6 +202,11 @@ def main():
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
     ap.add_argument("--sweep", action="store_true",
                     help="print recall@10 / QPS over an nprobe ladder and exit")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving mix over the index: Poisson arrivals, mixed k / nprobe / filters")
+    ap.add_argument("--serve-rates", default="5000,20000,50000,100000,200000",
+                    help="arrival rates (requests/s) of the serving run")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrivals per rate (seconds)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -232,6 +237,12 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, cfg, path, gm, gt, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    if args.serve:
+        run_serve(args, cfg, path, gm, gt, rank, world, local_rank)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -443,6 +454,65 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_serve(args, cfg, path, gm, gt, rank, world, local_rank):
+    """Serving mix over the index: Poisson arrivals at each rate of the ladder, k uniform in
+    {10, 20, 100}, nprobe uniform in {8, 32, 64}, half of the requests carrying one of 64
+    registered row-id filters of log-uniform selectivity in [0.001, 0.5]; continuous batching
+    over 3 contexts. Reports achieved QPS and p50 / p99 latency per rate, and the saturated QPS
+    (all requests queued at once) as the value."""
+    import torch
+    from pdx_b200 import compiled
+    from pdx_b200.serving import Server, make_filters, poisson_mix
+    ix = compiled.load_index(path, device=local_rank)
+    filters = make_filters(ix, 64, seed=5)
+    srv = Server(ix, max_batch=4096, n_contexts=3, k_max=100)
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    nmax = 200_000
+    Qall = gm.sample(nmax, 1 + rank)  # the first GT_QUERIES match the ground truth
+    # warm-up (allocations, module load) at saturation
+    srv.run(poisson_mix(Qall[:20_000], 0.0, filters, seed=4), realtime=False)
+    torch.cuda.synchronize()
+    ladder = []
+    sampler = ClockSampler(local_rank)
+    for rate in rates:
+        n = int(min(nmax, max(2000, rate * args.serve_seconds)))
+        w = poisson_mix(Qall[:n], rate, filters, seed=5)
+        out = srv.run(w, realtime=True)
+        ladder.append({"rate": rate, "requests": n, "qps": round(n / out.wall, 1),
+                       "p50_ms": round(float(np.percentile(out.latency, 50)) * 1e3, 3),
+                       "p99_ms": round(float(np.percentile(out.latency, 99)) * 1e3, 3),
+                       "batches": int(out.batch.max()) + 1})
+        log(f"serve rate {rate:.0f}/s: {ladder[-1]}")
+    w = poisson_mix(Qall, 0.0, filters, seed=5)
+    t_sat = []
+    for _ in range(max(1, args.steps // 10)):
+        out = srv.run(w, realtime=False)
+        t_sat.append(out.wall)
+    clocks = sampler.stop()
+    sat_qps = nmax / min(t_sat)
+    # recall@10 of the unfiltered requests that have ground truth
+    g = min(len(gt), nmax)
+    plain = np.nonzero(w.filter_id[:g] < 0)[0]
+    hits = 0
+    for i in plain:
+        ids_i, _ = out.result(i)
+        hits += len(set(ids_i[:10].tolist()) & set(gt[i, :10].tolist()))
+    rec10 = hits / (10 * max(1, len(plain)))
+    srv.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "served QPS (serving mix over the IVF2 SQ8 index)", "value": round(sat_qps, 1),
+            "unit": "queries/s", "n_gpus": world, "steps": len(t_sat), "warmup": 1,
+            "ms_per_step": round(1e3 * min(t_sat), 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded Gaussian mixture)",
+            "config": {"workload": f"serve_{args.config}", "requests_saturated": nmax,
+                       "k": [10, 20, 100], "nprobe": [8, 32, 64], "filtered_share": 0.5,
+                       "filters": "64 registered, selectivity log-uniform [0.001, 0.5]",
+                       "contexts": 3, "max_batch": 4096, "recall@10_unfiltered": round(rec10, 4),
+                       "ladder": ladder},
+            "clocks": clocks}), flush=True)
 
 
 def run_reference_arm(args, cfg, path, gm, gt, rank, world):

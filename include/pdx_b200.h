@@ -167,6 +167,47 @@ uint64_t pdxg_noalloc_scratch_bytes(void);
  * Results are identical in every mode. */
 int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
 
+/* ---------------------------------------------------------------------------------------
+ * Serving-style batches. A context owns a workspace and a CUDA stream; work issued on
+ * different contexts of one index runs concurrently. No counterpart in the reference (one
+ * query per call there); the per-query semantics are those of Search / FilteredSearch. */
+typedef struct pdxg_context pdxg_context;
+
+/* One request of a batch: k results (1 <= k <= k_max), nprobe as SetNProbe (0 = all
+ * clusters), and an optional filter: a registered filter (filter_id >= 0, see
+ * pdxg_filter_register) or else the row ids rows[filter_begin, filter_end) (filter_id = -1 and
+ * filter_begin = UINT64_MAX: no filter). */
+typedef struct {
+    uint32_t k;
+    uint32_t nprobe;
+    uint64_t filter_begin;
+    uint64_t filter_end;
+    int32_t filter_id;
+    uint32_t reserved;  /* 0 */
+} pdxg_request;
+
+int pdxg_context_create(pdxg_index* index, pdxg_context** out);
+void pdxg_context_free(pdxg_context* context);
+/* The context's cudaStream_t. */
+void* pdxg_context_stream(pdxg_context* context);
+
+/* Enqueues one batch on the context's stream and returns without waiting. `queries` (nq x d)
+ * and the outputs ids / distances (nq x k_max, row stride k_max) and counts (nq) are GPU
+ * memory; `requests` (nq) and `rows` (the filters' row ids) are host memory, staged before the
+ * call returns. Filters are built on the GPU as one bit per cluster slot. A second call on the
+ * same context waits for the first call's host-to-device copies only. */
+int pdxg_search_requests(pdxg_context* context, const float* queries, uint32_t nq,
+                         const pdxg_request* requests, const uint32_t* rows, uint32_t k_max,
+                         uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts);
+
+/* Registered filters: the selection bitmap and per-cluster passing counts of a row-id list
+ * (CreatePredicateEvaluator, index.hpp:436-446), built once and kept in GPU memory, so that
+ * requests naming it stage no row ids. Unknown row ids are ignored, repeated ones count once.
+ * Registering may synchronize the device when the filter pool grows. A filter may be released
+ * only once the batches that name it have completed. */
+int pdxg_filter_register(pdxg_index* index, const uint64_t* row_ids, uint64_t n, int32_t* filter_id);
+int pdxg_filter_release(pdxg_index* index, int32_t filter_id);
+
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);
 

@@ -72,6 +72,12 @@ def library() -> C.CDLL:
         fn("pdxg_num_embeddings", C.c_uint64, vp)
         fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
         fn("pdxg_get_stats", C.c_int, vp, _u64p)
+        fn("pdxg_context_create", C.c_int, vp, C.POINTER(vp))
+        fn("pdxg_context_free", None, vp)
+        fn("pdxg_context_stream", vp, vp)
+        fn("pdxg_search_requests", C.c_int, vp, vp, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, vp, vp, vp)
+        fn("pdxg_filter_register", C.c_int, vp, vp, C.c_uint64, C.POINTER(C.c_int32))
+        fn("pdxg_filter_release", C.c_int, vp, C.c_int32)
         _lib = lib
     return _lib
 
@@ -305,6 +311,18 @@ class PDXIndex:
     def set_threads_per_query(self, threads: int) -> None:
         _check(library().pdxg_set_threads_per_query(self._handle().ptr, int(threads)))
 
+    def register_filter(self, row_ids: np.ndarray) -> int:
+        """Keeps the filter of `row_ids` resident on the GPU (extension); returns its id for
+        requests of Context.search_requests."""
+        r = np.ascontiguousarray(row_ids, dtype=np.uint64)
+        out = C.c_int32()
+        _check(library().pdxg_filter_register(self._handle().ptr, C.c_void_p(r.ctypes.data), len(r),
+                                              C.byref(out)))
+        return int(out.value)
+
+    def release_filter(self, filter_id: int) -> None:
+        _check(library().pdxg_filter_release(self._handle().ptr, int(filter_id)))
+
     # -- persistence & getters -----------------------------------------------------------
     def save(self, path: str) -> None:
         _check(library().pdxg_save(self._handle().ptr, os.fsencode(path)))
@@ -346,6 +364,61 @@ class PDXIndex:
         if self._type in ("pdx_f32", "pdx_u8"):
             raise RuntimeError("Delete is not implemented in PDXIndex. Use PDXTreeIndex instead.")
         raise RuntimeError("Delete is not supported by the GPU engine yet")
+
+
+# pdxg_request (include/pdx_b200.h)
+# pdxg_request: a filter is a registered filter (filter_id >= 0) or else the row-id range
+# rows[filter_begin, filter_end) (filter_id = -1 and filter_begin = NO_FILTER: unfiltered)
+REQUEST_DTYPE = np.dtype([("k", np.uint32), ("nprobe", np.uint32), ("filter_begin", np.uint64),
+                          ("filter_end", np.uint64), ("filter_id", np.int32), ("reserved", np.uint32)])
+NO_FILTER = np.uint64(np.iinfo(np.uint64).max)
+
+
+def request_table(n: int) -> np.ndarray:
+    """n unfiltered requests (k and nprobe still to be filled in)."""
+    t = np.zeros(n, dtype=REQUEST_DTYPE)
+    t["filter_begin"] = NO_FILTER
+    t["filter_end"] = NO_FILTER
+    t["filter_id"] = -1
+    return t
+
+
+class Context:
+    """A workspace + CUDA stream of one index (pdxg_context): batches issued on different
+    contexts run concurrently."""
+
+    def __init__(self, index: "PDXIndex"):
+        self.index = index
+        out = C.c_void_p()
+        _check(library().pdxg_context_create(index.handle.ptr, C.byref(out)))
+        self.ptr = out
+
+    @property
+    def stream(self) -> int:
+        return int(library().pdxg_context_stream(self.ptr) or 0)
+
+    def search_requests(self, queries_ptr: int, nq: int, requests: np.ndarray, rows: Optional[np.ndarray],
+                        k_max: int, ids_ptr: int, dists_ptr: int, counts_ptr: int,
+                        transformed: bool = False) -> None:
+        """Enqueues a batch (device queries/outputs, host requests/rows) on this context."""
+        req = np.ascontiguousarray(requests, dtype=REQUEST_DTYPE)
+        rws = None if rows is None else np.ascontiguousarray(rows, dtype=np.uint32)
+        _check(library().pdxg_search_requests(
+            self.ptr, C.c_void_p(queries_ptr), nq, C.c_void_p(req.ctypes.data),
+            C.c_void_p(rws.ctypes.data if rws is not None and len(rws) else 0), k_max,
+            PDXG_QUERY_TRANSFORMED if transformed else 0, C.c_void_p(ids_ptr), C.c_void_p(dists_ptr),
+            C.c_void_p(counts_ptr)))
+
+    def close(self):
+        if getattr(self, "ptr", None) and self.ptr.value and _lib is not None:
+            _lib.pdxg_context_free(self.ptr)
+            self.ptr = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def load_index(path: str, device: int = 0) -> PDXIndex:

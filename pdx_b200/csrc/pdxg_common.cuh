@@ -63,7 +63,13 @@ struct SearchParams {
     uint32_t n_order;
     const uint32_t* sel_bits;    // optional: [n_filters x l1.sel_words] selection bitmaps
     const uint32_t* passing;     // optional: [n_filters x l1.nclusters] passing counts
-    const int32_t* filter_of;    // optional: [nq] filter slot per query, -1 = unfiltered
+    const int32_t* filter_of;    // optional: [nq] filter per query: -1 unfiltered, f >= 0 the
+                                 // batch's filter f, -2 - r the registered filter r
+    const uint32_t* reg_sel;     // registered filters: [slots x l1.sel_words] selection bitmaps
+    const uint32_t* reg_pass;    // registered filters: [slots x l1.nclusters] passing counts
+    const uint32_t* q_k;         // optional per-query k (<= k, the output row stride)
+    const uint32_t* q_nprobe;    // optional per-query resolved nprobe (<= nprobe)
+    const uint32_t* q_top;       // optional per-query tree top-level probe (<= top_nprobe)
     uint32_t* out_ids;           // [nq x k]
     float* out_dists;            // [nq x k]
     uint32_t* out_counts;        // [nq]

@@ -265,7 +265,22 @@ struct Workspace {
     uint64_t l1_order_cap = 0;
     uint32_t* d_l1_count = nullptr;
     uint64_t l1_count_cap = 0;
+    // per-query request parameters (pdxg_search_requests)
+    uint32_t* d_req = nullptr;  // q_k | q_nprobe | q_top | filter_of, nq each
+    uint64_t req_cap = 0;
+    unsigned long long* d_foff = nullptr;
+    uint64_t foff_cap = 0;
+    uint32_t* d_rows = nullptr;
+    uint64_t rows_cap = 0;
 };
+
+void free_workspace(Workspace& w) {
+    void* ptrs[] = {w.d_q, w.d_rq, w.d_norms, w.d_ids, w.d_dists, w.d_counts, w.d_queue, w.d_order,
+                    w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_l1_order,
+                    w.d_l1_count, w.d_req, w.d_foff, w.d_rows};
+    for (void* q : ptrs) cudaFree(q);
+    w = Workspace();
+}
 
 }  // namespace
 
@@ -286,6 +301,8 @@ struct pdxg_index {
     float* d_cent0 = nullptr;
     float* d_rot = nullptr;
     float* d_ratios = nullptr;
+    uint32_t* d_rid_cluster = nullptr;  // row id -> cluster (device copy, filters)
+    uint32_t* d_rid_pos = nullptr;      // row id -> position in its cluster
     float eps0 = 1.5f;
     uint32_t nprobe = 0;
     uint32_t threads = 0;
@@ -297,6 +314,13 @@ struct pdxg_index {
     cudaStream_t stats_stream = nullptr;
     Workspace ws;
     std::mutex mu;
+    // registered filters (pdxg_filter_register): resident selection bitmaps + passing counts,
+    // one slot each; reg_mu is held from a batch's validation through its launch
+    uint32_t* d_reg_sel = nullptr;   // [reg_cap x l1.sel_words]
+    uint32_t* d_reg_pass = nullptr;  // [reg_cap x l1 clusters]
+    uint32_t reg_cap = 0;
+    std::vector<uint8_t> reg_used;
+    std::mutex reg_mu;
 };
 
 namespace {
@@ -352,26 +376,11 @@ void free_index(pdxg_index* ix) {
     cudaFree(ix->d_cent0);
     cudaFree(ix->d_rot);
     cudaFree(ix->d_ratios);
-    Workspace& w = ix->ws;
-    cudaFree(w.d_q);
-    cudaFree(w.d_rq);
-    cudaFree(w.d_norms);
-    cudaFree(w.d_ids);
-    cudaFree(w.d_dists);
-    cudaFree(w.d_counts);
-    cudaFree(w.d_queue);
-    cudaFree(w.d_order);
-    cudaFree(w.d_sel);
-    cudaFree(w.d_pass);
-    cudaFree(w.d_filter_of);
-    cudaFree(w.d_stats);
-    cudaFree(w.d_top_order);
-    cudaFree(w.d_top_off);
-    cudaFree(w.d_top_lists);
-    cudaFree(w.d_top_count);
-    cudaFree(w.d_top_vals);
-    cudaFree(w.d_l1_order);
-    cudaFree(w.d_l1_count);
+    cudaFree(ix->d_rid_cluster);
+    cudaFree(ix->d_rid_pos);
+    cudaFree(ix->d_reg_sel);
+    cudaFree(ix->d_reg_pass);
+    free_workspace(ix->ws);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
 }
@@ -542,6 +551,13 @@ int load_from_bytes(const uint8_t* buf, uint64_t size, int device, pdxg_index** 
                 ix->rid_pos[rid] = p;
             }
         }
+    if (cudaMalloc(&ix->d_rid_cluster, std::max<size_t>(total, 1) * 4) != cudaSuccess ||
+        cudaMalloc(&ix->d_rid_pos, std::max<size_t>(total, 1) * 4) != cudaSuccess ||
+        (total && cudaMemcpy(ix->d_rid_cluster, ix->rid_cluster.data(), total * 4, cudaMemcpyHostToDevice) != cudaSuccess) ||
+        (total && cudaMemcpy(ix->d_rid_pos, ix->rid_pos.data(), total * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
+        free_index(ix);
+        return fail(PDXG_ERR_CUDA, "cannot upload the row id map");
+    }
     // file buffer pointers are not kept
     for (HostLevel* lv : {&ix->l1, &ix->l0})
         for (FileCluster& f : lv->fc) {
@@ -560,7 +576,7 @@ struct Launch {
 };
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
-                Launch& L) {
+                Launch& L, uint32_t np_flat_max = 0xFFFFFFFFu, uint32_t top_max = 0xFFFFFFFFu) {
     SearchParams& p = L.p;
     p.arena = ix->arena;
     p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale);
@@ -571,13 +587,16 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
     p.k = k;
     const uint32_t n1 = p.l1.nclusters;
     // flat: searcher.hpp:614-616; tree: index.hpp:546-556
-    const uint32_t np_flat = (ix->nprobe == 0 || ix->nprobe > n1) ? n1 : ix->nprobe;
+    uint32_t np_flat = (ix->nprobe == 0 || ix->nprobe > n1) ? n1 : ix->nprobe;
     uint32_t top = 0;
     if (ix->tree) {
         top = p.l0.nclusters;
         const uint32_t l1np = ix->nprobe == 0 ? n1 : ix->nprobe;
         if (l1np < n1 / 2) top /= 2;
     }
+    // per-query batches (pdxg_search_requests) size everything for their largest values
+    if (np_flat_max != 0xFFFFFFFFu) np_flat = np_flat_max;
+    if (top_max != 0xFFFFFFFFu) top = top_max;
     p.nprobe = np_flat;
     p.top_nprobe = top;
     p.n_order = n_order;
@@ -619,8 +638,7 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
     return PDXG_OK;
 }
 
-int ensure_ws(pdxg_index* ix, uint32_t nq, uint32_t k) {
-    Workspace& w = ix->ws;
+int ensure_ws(pdxg_index* ix, Workspace& w, uint32_t nq, uint32_t k) {
     uint64_t cap;
     if (nq > w.q_cap || !w.d_rq) {
         cap = 0;
@@ -650,7 +668,7 @@ int ensure_ws(pdxg_index* ix, uint32_t nq, uint32_t k) {
 // Tree top level as its own launch of small CTAs (top_level_kernel): on success the search
 // kernel reads each query's L1 order from L.p.q_order; in the per-query mode the search kernel
 // runs the top level itself.
-int run_top_level(pdxg_index* ix, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
     if (ix->top_mode == 1) return PDXG_OK;
@@ -680,7 +698,6 @@ int run_top_level(pdxg_index* ix, const float* qp, uint32_t nq, Launch& L, cudaS
         if (ix->top_mode == 2) return fail(PDXG_ERR_CAPACITY, "top-level kernel does not fit in shared memory");
         return PDXG_OK;
     }
-    Workspace& w = ix->ws;
     int rc;
     if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
     if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
@@ -700,7 +717,7 @@ int run_top_level(pdxg_index* ix, const float* qp, uint32_t nq, Launch& L, cudaS
 }
 
 // Core device-side search: queries/ids/dists/counts are device pointers.
-int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, uint32_t flags,
+int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, uint32_t k, uint32_t flags,
                        const uint32_t* d_order, uint32_t n_order, const uint32_t* d_sel,
                        const uint32_t* d_pass, const int32_t* d_filter_of, bool any_filter,
                        uint32_t* ids, float* dists, uint32_t* counts, cudaStream_t st) {
@@ -709,13 +726,13 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
         PDXG_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, st));
         return PDXG_OK;
     }
-    int rc = ensure_ws(ix, nq, k);
+    int rc = ensure_ws(ix, w, nq, k);
     if (rc) return rc;
     const float* qp = q;
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
-        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, ix->ws.d_norms,
-                                         ix->ws.d_rq, st));
-        qp = ix->ws.d_rq;
+        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, w.d_norms,
+                                         w.d_rq, st));
+        qp = w.d_rq;
     }
     Launch L;
     rc = plan_search(ix, nq, k, n_order, any_filter, L);
@@ -728,19 +745,19 @@ int search_device_impl(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k, 
     L.p.out_ids = ids;
     L.p.out_dists = dists;
     L.p.out_counts = counts;
-    L.p.queue = ix->ws.d_queue;
+    L.p.queue = w.d_queue;
     L.p.stats = nullptr;
     if (flags & PDXG_COLLECT_STATS) {
-        if (!ix->ws.d_stats) PDXG_CUDA(cudaMalloc(&ix->ws.d_stats, 12 * sizeof(unsigned long long)));
-        PDXG_CUDA(cudaMemsetAsync(ix->ws.d_stats, 0, 12 * sizeof(unsigned long long), st));
-        L.p.stats = ix->ws.d_stats;
+        if (!w.d_stats) PDXG_CUDA(cudaMalloc(&w.d_stats, 12 * sizeof(unsigned long long)));
+        PDXG_CUDA(cudaMemsetAsync(w.d_stats, 0, 12 * sizeof(unsigned long long), st));
+        L.p.stats = w.d_stats;
         ix->stats_stream = st;
     }
     if (ix->tree && !any_filter && !d_order) {
-        rc = run_top_level(ix, qp, nq, L, st);
+        rc = run_top_level(ix, w, qp, nq, L, st);
         if (rc) return rc;
     }
-    PDXG_CUDA(cudaMemsetAsync(ix->ws.d_queue, 0, sizeof(uint32_t), st));
+    PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     return PDXG_OK;
 }
@@ -797,7 +814,7 @@ int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t
     if (!queries || !ids || !dists || !counts)
         return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
     PDXG_CUDA(cudaSetDevice(ix->device));
-    int rc = ensure_ws(ix, nq, k);
+    int rc = ensure_ws(ix, ix->ws, nq, k);
     if (rc) return rc;
     Workspace& w = ix->ws;
     cudaStream_t st = ix->stream;
@@ -829,7 +846,7 @@ int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t
         d_pass = w.d_pass;
         d_fo = w.d_filter_of;
     }
-    rc = search_device_impl(ix, w.d_q, nq, k, flags, d_order, n_order, d_sel, d_pass, d_fo,
+    rc = search_device_impl(ix, w, w.d_q, nq, k, flags, d_order, n_order, d_sel, d_pass, d_fo,
                             any_filter, w.d_ids, w.d_dists, w.d_counts, st);
     if (rc) return rc;
     PDXG_CUDA(cudaMemcpyAsync(ids, w.d_ids, sizeof(uint32_t) * nq * k, cudaMemcpyDeviceToHost, st));
@@ -934,7 +951,7 @@ int pdxg_search_device(pdxg_index* ix, const float* queries, uint32_t nq, uint32
     std::lock_guard<std::mutex> lock(ix->mu);
     PDXG_CUDA(cudaSetDevice(ix->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ix->stream;
-    return search_device_impl(ix, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr,
+    return search_device_impl(ix, ix->ws, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr,
                               false, ids, distances, counts, st);
 }
 
@@ -1003,7 +1020,7 @@ int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, floa
     if (!queries || !out) return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
     std::lock_guard<std::mutex> lock(ix->mu);
     PDXG_CUDA(cudaSetDevice(ix->device));
-    int rc = ensure_ws(ix, nq, 1);
+    int rc = ensure_ws(ix, ix->ws, nq, 1);
     if (rc) return rc;
     cudaStream_t st = ix->stream;
     PDXG_CUDA(cudaMemcpyAsync(ix->ws.d_q, queries, sizeof(float) * nq * ix->d, cudaMemcpyHostToDevice, st));
@@ -1123,6 +1140,278 @@ int pdxg_save(pdxg_index* ix, const char* path) {
         out.write(reinterpret_cast<const char*>(&ix->scale), 4);
     }
     if (!out) return fail(PDXG_ERR_IO, std::string("Failed to write file: ") + path);
+    return PDXG_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================== request batches
+// Serving-style batches: every query carries its own k, nprobe and optional row-id filter.
+// A context owns one workspace and one stream, so batches issued on different contexts run
+// concurrently on the GPU without sharing scratch.
+
+struct pdxg_context {
+    pdxg_index* ix = nullptr;
+    Workspace ws;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t staged = nullptr;   // the previous call's host-to-device copies are done
+    bool staged_pending = false;
+    uint8_t* h_stage = nullptr;     // pinned staging of the per-query parameters and rows
+    size_t h_cap = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+// One bit per cluster slot: filter f selects row r when bit pos(r) of cluster(r) is set;
+// passing[f][c] counts distinct selected rows (CreatePredicateEvaluator, index.hpp:436-446).
+__global__ void build_filters_kernel(const uint32_t* __restrict__ rows,
+                                     const unsigned long long* __restrict__ foff, uint32_t nf,
+                                     const uint32_t* __restrict__ rid_cluster,
+                                     const uint32_t* __restrict__ rid_pos, uint64_t n_rows,
+                                     const DevCluster* __restrict__ clusters, uint32_t words,
+                                     uint32_t ncl, uint32_t* sel, uint32_t* passing) {
+    const uint32_t f = blockIdx.y;
+    if (f >= nf) return;
+    const unsigned long long a = foff[f], b = foff[f + 1];
+    for (unsigned long long i = a + blockIdx.x * blockDim.x + threadIdx.x; i < b;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t r = rows[i];
+        if (r >= n_rows) continue;
+        const uint32_t c = rid_cluster[r];
+        if (c == 0xFFFFFFFFu) continue;
+        const uint32_t pos = rid_pos[r];
+        const uint32_t bit = 1u << (pos & 31);
+        const uint32_t old = atomicOr(sel + (size_t)f * words + clusters[c].sel_word + (pos >> 5), bit);
+        if (!(old & bit)) atomicAdd(passing + (size_t)f * ncl + c, 1u);
+    }
+}
+
+int stage_grow(pdxg_context* ctx, size_t need) {
+    if (need <= ctx->h_cap) return PDXG_OK;
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    ctx->h_stage = nullptr;
+    ctx->h_cap = 0;
+    PDXG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_stage), need, cudaHostAllocDefault));
+    ctx->h_cap = need;
+    return PDXG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pdxg_context_create(pdxg_index* ix, pdxg_context** out) {
+    if (int rc = check_index(ix)) return rc;
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    auto* ctx = new pdxg_context();
+    ctx->ix = ix;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->staged, cudaEventDisableTiming) != cudaSuccess) {
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return fail(PDXG_ERR_CUDA, "cannot create the context's stream");
+    }
+    *out = ctx;
+    return PDXG_OK;
+}
+
+void pdxg_context_free(pdxg_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->ix->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_workspace(ctx->ws);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    cudaEventDestroy(ctx->staged);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+void* pdxg_context_stream(pdxg_context* ctx) { return ctx ? ctx->stream : nullptr; }
+
+int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
+                         const pdxg_request* requests, const uint32_t* rows, uint32_t k_max,
+                         uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts) {
+    if (!ctx) return fail(PDXG_ERR_INVALID_ARGUMENT, "context is NULL");
+    pdxg_index* ix = ctx->ix;
+    if (!queries || !requests || !ids || !distances || !counts)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (flags & PDXG_COLLECT_STATS) return fail(PDXG_ERR_INVALID_ARGUMENT, "stats are not collected here");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    cudaStream_t st = ctx->stream;
+    if (nq == 0) return PDXG_OK;
+    // the registry cannot grow (and move) between the checks below and the launch
+    std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
+    // resolve every query's parameters as PDXearch / PDXTreeIndex::Search would
+    const uint32_t n1 = (uint32_t)ix->l1.fc.size();
+    const uint32_t n0 = (uint32_t)ix->l0.fc.size();
+    uint32_t np_max = 1, top_max = 0, nf = 0;
+    uint64_t nrows = 0;
+    bool any_filter = false, any_plain = false;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const pdxg_request& r = requests[q];
+        if (r.k == 0 || r.k > k_max) return fail(PDXG_ERR_INVALID_ARGUMENT, "request k must be in [1, k_max]");
+        if (r.filter_id >= 0) {
+            if ((uint32_t)r.filter_id >= ix->reg_cap || !ix->reg_used[r.filter_id])
+                return fail(PDXG_ERR_INVALID_ARGUMENT, "unknown filter id " + std::to_string(r.filter_id));
+            any_filter = true;
+        } else if (r.filter_id != -1) {
+            return fail(PDXG_ERR_INVALID_ARGUMENT, "filter_id must be -1 or a registered filter");
+        } else if (r.filter_begin != UINT64_MAX) {
+            if (r.filter_end < r.filter_begin) return fail(PDXG_ERR_INVALID_ARGUMENT, "bad filter range");
+            if (r.filter_end > r.filter_begin && !rows) return fail(PDXG_ERR_INVALID_ARGUMENT, "rows is NULL");
+            ++nf;
+            nrows += r.filter_end - r.filter_begin;
+            any_filter = true;
+        } else {
+            any_plain = true;
+        }
+    }
+    // pinned staging: q_k, q_np, q_top, filter_of (nq each), filter offsets (nf + 1), rows
+    const size_t req_bytes = (size_t)nq * 16, foff_bytes = ((size_t)nf + 1) * 8, row_bytes = nrows * 4;
+    if (ctx->staged_pending) PDXG_CUDA(cudaEventSynchronize(ctx->staged));
+    int rc = stage_grow(ctx, req_bytes + foff_bytes + row_bytes + 64);
+    if (rc) return rc;
+    uint32_t* h_req = reinterpret_cast<uint32_t*>(ctx->h_stage);
+    unsigned long long* h_foff = reinterpret_cast<unsigned long long*>(ctx->h_stage + req_bytes);
+    uint32_t* h_rows = reinterpret_cast<uint32_t*>(ctx->h_stage + req_bytes + foff_bytes);
+    uint32_t f = 0;
+    unsigned long long pos = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const pdxg_request& r = requests[q];
+        const uint32_t npf = (r.nprobe == 0 || r.nprobe > n1) ? n1 : r.nprobe;
+        uint32_t top = 0;
+        if (ix->tree) {
+            top = n0;
+            if ((r.nprobe == 0 ? n1 : r.nprobe) < n1 / 2) top /= 2;
+        }
+        h_req[q] = r.k;
+        h_req[nq + q] = npf;
+        h_req[2 * nq + q] = top;
+        np_max = std::max(np_max, npf);
+        top_max = std::max(top_max, top);
+        if (r.filter_id >= 0) {
+            h_req[3 * nq + q] = (uint32_t)(-2 - r.filter_id);
+        } else if (r.filter_begin != UINT64_MAX) {
+            h_req[3 * nq + q] = f;
+            h_foff[f] = pos;
+            const uint64_t len = r.filter_end - r.filter_begin;
+            const uint32_t* src = rows + r.filter_begin;
+            std::memcpy(h_rows + pos, src, len * 4);
+            pos += len;
+            ++f;
+        } else {
+            h_req[3 * nq + q] = 0xFFFFFFFFu;  // -1: unfiltered
+        }
+    }
+    h_foff[nf] = pos;
+    Workspace& w = ctx->ws;
+    if ((rc = ensure_ws(ix, w, nq, k_max))) return rc;
+    if ((rc = dev_grow(w.d_req, w.req_cap, (uint64_t)nq * 4))) return rc;
+    if ((rc = dev_grow(w.d_foff, w.foff_cap, (uint64_t)nf + 1))) return rc;
+    if ((rc = dev_grow(w.d_rows, w.rows_cap, std::max<uint64_t>(nrows, 1)))) return rc;
+    PDXG_CUDA(cudaMemcpyAsync(w.d_req, h_req, req_bytes, cudaMemcpyHostToDevice, st));
+    if (nf) {
+        PDXG_CUDA(cudaMemcpyAsync(w.d_foff, h_foff, foff_bytes, cudaMemcpyHostToDevice, st));
+        if (nrows) PDXG_CUDA(cudaMemcpyAsync(w.d_rows, h_rows, row_bytes, cudaMemcpyHostToDevice, st));
+    }
+    PDXG_CUDA(cudaEventRecord(ctx->staged, st));
+    ctx->staged_pending = true;
+    const uint32_t words = ix->l1.sel_words;
+    if (nf) {
+        if ((rc = dev_grow(w.d_sel, w.sel_cap, (uint64_t)nf * words))) return rc;
+        if ((rc = dev_grow(w.d_pass, w.pass_cap, (uint64_t)nf * n1))) return rc;
+        PDXG_CUDA(cudaMemsetAsync(w.d_sel, 0, (size_t)nf * words * 4, st));
+        PDXG_CUDA(cudaMemsetAsync(w.d_pass, 0, (size_t)nf * n1 * 4, st));
+        uint64_t max_len = 0;
+        for (uint32_t i = 0; i < nf; ++i) max_len = std::max<uint64_t>(max_len, h_foff[i + 1] - h_foff[i]);
+        dim3 grid((uint32_t)std::min<uint64_t>((max_len + 255) / 256 + 1, 64), nf);
+        build_filters_kernel<<<grid, 256, 0, st>>>(w.d_rows, w.d_foff, nf, ix->d_rid_cluster, ix->d_rid_pos,
+                                                   ix->rid_cluster.size(), ix->d_cl1, words, n1, w.d_sel,
+                                                   w.d_pass);
+        PDXG_CUDA(cudaGetLastError());
+    }
+    const float* qp = queries;
+    if (!(flags & PDXG_QUERY_TRANSFORMED)) {
+        PDXG_CUDA(launch_prepare_queries(queries, nq, ix->d, ix->d_rot, ix->normalized, w.d_norms, w.d_rq, st));
+        qp = w.d_rq;
+    }
+    Launch L;
+    if ((rc = plan_search(ix, nq, k_max, 0, any_filter, L, np_max, top_max))) return rc;
+    L.p.queries = qp;
+    L.p.q_k = w.d_req;
+    L.p.q_nprobe = w.d_req + nq;
+    L.p.q_top = w.d_req + 2 * nq;
+    if (any_filter) {
+        L.p.filter_of = reinterpret_cast<const int32_t*>(w.d_req + 3 * nq);
+        L.p.sel_bits = nf ? w.d_sel : nullptr;
+        L.p.passing = nf ? w.d_pass : nullptr;
+        L.p.reg_sel = ix->d_reg_sel;
+        L.p.reg_pass = ix->d_reg_pass;
+    }
+    L.p.out_ids = ids;
+    L.p.out_dists = distances;
+    L.p.out_counts = counts;
+    L.p.queue = w.d_queue;
+    if (ix->tree && any_plain) {
+        if ((rc = run_top_level(ix, w, qp, nq, L, st))) return rc;
+    }
+    PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
+    PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
+    return PDXG_OK;
+}
+
+int pdxg_filter_register(pdxg_index* ix, const uint64_t* row_ids, uint64_t n, int32_t* filter_id) {
+    if (int rc = check_index(ix)) return rc;
+    if (!filter_id) return fail(PDXG_ERR_INVALID_ARGUMENT, "filter_id is NULL");
+    if (n && !row_ids) return fail(PDXG_ERR_INVALID_ARGUMENT, "row_ids is NULL");
+    std::lock_guard<std::mutex> lock(ix->reg_mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    const uint32_t words = ix->l1.sel_words;
+    const uint32_t n1 = (uint32_t)ix->l1.fc.size();
+    uint32_t slot = 0;
+    while (slot < ix->reg_cap && ix->reg_used[slot]) ++slot;
+    if (slot == ix->reg_cap) {
+        if (ix->reg_cap >= (1u << 30)) return fail(PDXG_ERR_CAPACITY, "too many registered filters");
+        const uint32_t cap = std::max(8u, ix->reg_cap * 2);
+        uint32_t *sel = nullptr, *pass = nullptr;
+        if (cudaMalloc(&sel, (size_t)cap * words * 4) != cudaSuccess ||
+            cudaMalloc(&pass, (size_t)cap * n1 * 4) != cudaSuccess) {
+            cudaFree(sel);
+            return fail(PDXG_ERR_CUDA, "cannot grow the filter pool");
+        }
+        // batches already enqueued may still read the old pool: finish them before freeing it
+        PDXG_CUDA(cudaDeviceSynchronize());
+        if (ix->reg_cap) {
+            PDXG_CUDA(cudaMemcpy(sel, ix->d_reg_sel, (size_t)ix->reg_cap * words * 4, cudaMemcpyDeviceToDevice));
+            PDXG_CUDA(cudaMemcpy(pass, ix->d_reg_pass, (size_t)ix->reg_cap * n1 * 4, cudaMemcpyDeviceToDevice));
+        }
+        cudaFree(ix->d_reg_sel);
+        cudaFree(ix->d_reg_pass);
+        ix->d_reg_sel = sel;
+        ix->d_reg_pass = pass;
+        ix->reg_cap = cap;
+        ix->reg_used.resize(cap, 0);
+    }
+    std::vector<uint32_t> sel(words, 0), pass(n1, 0);
+    build_filter(ix, row_ids, n, sel.data(), pass.data());
+    PDXG_CUDA(cudaMemcpy(ix->d_reg_sel + (size_t)slot * words, sel.data(), (size_t)words * 4,
+                         cudaMemcpyHostToDevice));
+    PDXG_CUDA(cudaMemcpy(ix->d_reg_pass + (size_t)slot * n1, pass.data(), (size_t)n1 * 4,
+                         cudaMemcpyHostToDevice));
+    ix->reg_used[slot] = 1;
+    *filter_id = (int32_t)slot;
+    return PDXG_OK;
+}
+
+int pdxg_filter_release(pdxg_index* ix, int32_t filter_id) {
+    if (int rc = check_index(ix)) return rc;
+    std::lock_guard<std::mutex> lock(ix->reg_mu);
+    if (filter_id < 0 || (uint32_t)filter_id >= ix->reg_cap || !ix->reg_used[filter_id])
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "unknown filter id " + std::to_string(filter_id));
+    ix->reg_used[filter_id] = 0;
     return PDXG_OK;
 }
 

@@ -66,12 +66,21 @@ struct LevelOps {
     const DevLevel& lv;
     Shared& sh;
     Scalars& s;
-    int filter;      // -1 = unfiltered
-    bool top_level;  // the tree's meso-cluster search
+    const uint32_t* fsel;   // this query's selection bitmap over the level (null = unfiltered)
+    const uint32_t* fpass;  // this query's passing count per cluster
+    bool top_level;         // the tree's meso-cluster search
 
     __device__ LevelOps(const SearchParams& p_, const DevLevel& lv_, Shared& sh_, Scalars& s_,
-                        int filter_, bool top_level_ = false)
-        : p(p_), lv(lv_), sh(sh_), s(s_), filter(filter_), top_level(top_level_) {}
+                        int filter, bool top_level_ = false)
+        : p(p_), lv(lv_), sh(sh_), s(s_), fsel(nullptr), fpass(nullptr), top_level(top_level_) {
+        if (filter >= 0) {
+            fsel = p.sel_bits + (size_t)filter * lv.sel_words;
+            fpass = p.passing + (size_t)filter * lv.nclusters;
+        } else if (filter <= -2) {
+            fsel = p.reg_sel + (size_t)(-2 - filter) * lv.sel_words;
+            fpass = p.reg_pass + (size_t)(-2 - filter) * lv.nclusters;
+        }
+    }
 
     __device__ __forceinline__ const uint32_t* vert(const DevCluster& c) const {
         return reinterpret_cast<const uint32_t*>(p.arena + c.vert_off);
@@ -98,8 +107,8 @@ struct LevelOps {
         return u8 ? raw < thr : __uint_as_float(raw) < __uint_as_float(thr);
     }
     __device__ __forceinline__ bool selected(const DevCluster& c, uint32_t v) const {
-        if (filter < 0) return true;
-        const uint32_t* bits = p.sel_bits + (size_t)filter * lv.sel_words + c.sel_word;
+        if (!fsel) return true;
+        const uint32_t* bits = fsel + c.sel_word;
         return (__ldg(bits + (v >> 5)) >> (v & 31)) & 1u;
     }
     // Algorithmic-traffic accounting (only when p.stats is set; values are block-uniform).
@@ -407,7 +416,7 @@ struct LevelOps {
         uint32_t cur = 0;
         zero_dist(n);
         bool skip_warmup = false;
-        if (filter >= 0) {
+        if (fsel) {
             const uint32_t mask = mask_raw();
             for (uint32_t v = threadIdx.x; v < n; v += T)
                 if (!selected(c, v)) sh.dist[v] = mask;
@@ -526,8 +535,8 @@ struct LevelOps {
             const uint32_t cidx = sh.order[ci];
             const DevCluster c = lv.clusters[cidx];
             uint32_t passing = 0;
-            if (filter >= 0) {
-                passing = __ldg(p.passing + (size_t)filter * lv.nclusters + cidx);
+            if (fsel) {
+                passing = __ldg(fpass + cidx);
                 if (passing == 0) continue;
             }
             if (c.n == 0) continue;
@@ -535,7 +544,7 @@ struct LevelOps {
             if (s.hsize < k) {
                 long long t0 = 0;
                 if (p.stats && threadIdx.x == 0) t0 = clock64();
-                if (filter >= 0)
+                if (fsel)
                     filtered_start(c, k, passing);
                 else
                     start(c, k);
@@ -669,32 +678,36 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
 
         long long t_q0 = 0;
         if (p.stats && threadIdx.x == 0) t_q0 = clock64();
+        // per-query parameters (serving batches mix them); p.k is the output row stride
+        const uint32_t kq = p.q_k ? __ldg(p.q_k + q) : p.k;
+        const uint32_t npq = p.q_nprobe ? __ldg(p.q_nprobe + q) : p.nprobe;
+        const uint32_t topq = p.q_top ? __ldg(p.q_top + q) : p.top_nprobe;
         uint32_t nvisit;
         if (p.order) {
             // caller-provided access order (PDXearch::SetClusterAccessOrder, searcher.hpp:48-54)
-            nvisit = p.nprobe < p.n_order ? p.nprobe : p.n_order;
+            nvisit = npq < p.n_order ? npq : p.n_order;
             for (uint32_t i = threadIdx.x; i < nvisit; i += T) sh.order[i] = __ldg(p.order + i);
             __syncthreads();
-        } else if (p.is_tree && filter < 0 && p.q_order) {
+        } else if (p.is_tree && filter == -1 && p.q_order) {
             // batched tree top level (pdxg_toplevel.cu) already produced this query's L1 order
             nvisit = __ldg(p.q_order_count + q);
             for (uint32_t i = threadIdx.x; i < nvisit; i += T)
                 sh.order[i] = __ldg(p.q_order + (size_t)q * p.q_order_stride + i);
             __syncthreads();
-        } else if (p.is_tree && filter < 0) {
+        } else if (p.is_tree && filter == -1) {
             // PDXTreeIndex::Search (index.hpp:545-566): pruned F32 search over the meso
             // clusters with k = nprobe returns the L1 clusters to visit, nearest first.
             LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
-            const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
-            top.probe(p.top_nprobe);
-            top.run(p.nprobe, nv0);
-            const uint32_t cnt = top.sort_heap(p.nprobe);
+            const uint32_t nv0 = topq < p.l0.nclusters ? topq : p.l0.nclusters;
+            top.probe(topq);
+            top.run(npq, nv0);
+            const uint32_t cnt = top.sort_heap(npq);
             for (uint32_t i = threadIdx.x; i < cnt; i += T) sh.order[i] = (uint32_t)sh.sortw[i];
             __syncthreads();
             nvisit = cnt;
         } else {
             LevelOps<T, false> probe_ops(p, p.l1, sh, s, -1);
-            nvisit = probe_ops.probe(p.nprobe);
+            nvisit = probe_ops.probe(npq);
         }
 
         if (p.stats && threadIdx.x == 0) {
@@ -703,8 +716,8 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             t_q0 = now;
         }
         LevelOps<T, U8> ops(p, p.l1, sh, s, filter);
-        ops.run(p.k, nvisit);
-        const uint32_t cnt = ops.sort_heap(p.k);
+        ops.run(kq, nvisit);
+        const uint32_t cnt = ops.sort_heap(kq);
         uint32_t* oi = p.out_ids + (size_t)q * p.k;
         float* od = p.out_dists + (size_t)q * p.k;
         for (uint32_t i = threadIdx.x; i < p.k; i += T) {
@@ -764,6 +777,11 @@ __global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ Se
         const uint32_t q = s.query;
         __syncthreads();
         if (q >= p.nq) break;
+        if (p.filter_of && __ldg(p.filter_of + q) != -1) {
+            // filtered queries probe the L1 centroids directly (no top-level search)
+            if (threadIdx.x == 0) out_count[q] = 0;
+            continue;
+        }
         if (threadIdx.x == 0) {
             for (int i = 0; i < 6; ++i) s.bytes[i] = 0;
             s.visits = 0;
@@ -773,10 +791,12 @@ __global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ Se
         for (uint32_t i = threadIdx.x; i < p.l0.d; i += T) sh.qf[i] = __ldg(src + i);
         __syncthreads();
         LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
-        const uint32_t nv0 = p.top_nprobe < p.l0.nclusters ? p.top_nprobe : p.l0.nclusters;
-        top.probe(p.top_nprobe);
-        top.run(p.nprobe, nv0);
-        const uint32_t cnt = top.sort_heap(p.nprobe);
+        const uint32_t npq = p.q_nprobe ? __ldg(p.q_nprobe + q) : p.nprobe;
+        const uint32_t topq = p.q_top ? __ldg(p.q_top + q) : p.top_nprobe;
+        const uint32_t nv0 = topq < p.l0.nclusters ? topq : p.l0.nclusters;
+        top.probe(topq);
+        top.run(npq, nv0);
+        const uint32_t cnt = top.sort_heap(npq);
         for (uint32_t i = threadIdx.x; i < cnt; i += T)
             out_order[(size_t)q * p.q_order_stride + i] = (uint32_t)sh.sortw[i];
         if (threadIdx.x == 0) {
