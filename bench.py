@@ -326,24 +326,26 @@ def main():
     ix.search_device(prepared.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
                      cnt_dev.data_ptr(), stream=sp, transformed=True, stats=True)
     stats = ix.last_stats()
-    kev = []
+    # the scan kernel alone: events the engine records around its own launches on `stream`
+    times = []
     for i in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        ix.search_device(prepared.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
-                         cnt_dev.data_ptr(), stream=sp, transformed=True)
-        b.record(stream)
+        ix.search_device(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
+                         cnt_dev.data_ptr(), stream=sp, time_kernels=True)
+        times.append(ix.kernel_times())
         flush.zero_()
-        kev.append((a, b))
     torch.cuda.synchronize()
-    kern_ms = statistics.mean(a.elapsed_time(b) for a, b in kev)
+    kern_ms = statistics.mean(t["scan"] for t in times)
+    top_ms = statistics.mean(t["top_level"] for t in times)
+    prep_ms = statistics.mean(t["prepare"] for t in times)
+    bp = stats["bytes_by_phase"]
+    scan_bytes = bp["start"] + bp["warmup"] + bp["survivor_horizontal"] + bp["survivor_vertical"] + bp["probe"]
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak = float(json.load(open(peaks_path))["hbm_gbs"])
         peak_src = "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    achieved = stats["bytes"] / (kern_ms / 1e3) / 1e9
+    achieved = scan_bytes / (kern_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -440,7 +442,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": "search_kernel", "kernel_ms": round(kern_ms, 3),
-                         "algorithmic_bytes_per_launch": stats["bytes"], "peak_source": peak_src,
+                         "algorithmic_bytes_per_launch": scan_bytes, "peak_source": peak_src,
+                         "other_kernels_ms": {"top_level_kernel": round(top_ms, 3),
+                                              "query_norms + rotation": round(prep_ms, 3)},
+                         "top_level_bytes_l2_resident": bp["top_level"],
                          "clusters_visited": stats["clusters_visited"],
                          "bytes_by_phase": stats["bytes_by_phase"],
                          "cycles_by_phase": stats["cycles_by_phase"]},
@@ -448,7 +453,8 @@ def main():
             "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * d * 4,
                     "d2h_bytes_per_step": nq * k * 8 + nq * 4},
-            "gpu_launches": 3 * args.steps if cfg["normalize"] else 2 * args.steps,
+            # per step: [query norms] + rotation + [tree top level] + scan
+            "gpu_launches": args.steps * ((2 if cfg["normalize"] else 1) + (1 if "tree" in cfg["itype"] else 0) + 1),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -46,6 +46,9 @@ typedef struct pdxg_index pdxg_index;
 #define PDXG_COLLECT_STATS 2u     /* count the index bytes the search algorithm reads (centroid
                                      probes, Start scans, warmup steps, survivor gathers);
                                      read them back with pdxg_get_stats */
+#define PDXG_TIME_KERNELS 4u      /* record CUDA events around the query preparation, the tree
+                                     top level and the scan kernel on the search's stream;
+                                     read the durations with pdxg_kernel_times */
 
 /* Last error message of the calling thread (never NULL). */
 const char* pdxg_last_error(void);
@@ -132,6 +135,12 @@ int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, f
  * the rest of the scan. No counterpart in the reference (its profiler times phases, profiler.hpp:36-320);
  * used for the roofline accounting. */
 int pdxg_get_stats(pdxg_index* index, uint64_t out[12]);
+
+/* Durations (ms) of the last search launched with PDXG_TIME_KERNELS through pdxg_search_device:
+ * out[0] query preparation (normalization + rotation), out[1] tree top level, out[2] the scan
+ * kernel (0 for a stage that did not run). Waits for that search to finish. No counterpart in
+ * the reference; used for the roofline accounting. */
+int pdxg_kernel_times(pdxg_index* index, float out[3]);
 
 /* Size of the fixed scratch array behind pdxg_search_device_noalloc, per GPU. */
 #define PDXG_NOALLOC_SCRATCH_BYTES (8u << 20)

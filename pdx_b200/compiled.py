@@ -25,6 +25,7 @@ PDXG_OK = 0
 PDXG_ERR_INVALID_ARGUMENT = 1
 PDXG_QUERY_TRANSFORMED = 1
 PDXG_COLLECT_STATS = 2
+PDXG_TIME_KERNELS = 4
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -72,6 +73,7 @@ def library() -> C.CDLL:
         fn("pdxg_num_embeddings", C.c_uint64, vp)
         fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
         fn("pdxg_get_stats", C.c_int, vp, _u64p)
+        fn("pdxg_kernel_times", C.c_int, vp, _f32p)
         fn("pdxg_context_create", C.c_int, vp, C.POINTER(vp))
         fn("pdxg_context_free", None, vp)
         fn("pdxg_context_stream", vp, vp)
@@ -286,9 +288,10 @@ class PDXIndex:
 
     def search_device(self, queries_ptr: int, nq: int, knn: int, ids_ptr: int, dists_ptr: int,
                       counts_ptr: int, stream: int = 0, transformed: bool = False,
-                      stats: bool = False) -> None:
+                      stats: bool = False, time_kernels: bool = False) -> None:
         """Enqueues a search on GPU-resident buffers (raw device pointers) on `stream`."""
         flags = (PDXG_QUERY_TRANSFORMED if transformed else 0) | (PDXG_COLLECT_STATS if stats else 0)
+        flags |= PDXG_TIME_KERNELS if time_kernels else 0
         _check(library().pdxg_search_device(self._handle().ptr, C.c_void_p(queries_ptr), nq, knn,
                                             flags, C.c_void_p(ids_ptr), C.c_void_p(dists_ptr),
                                             C.c_void_p(counts_ptr), C.c_void_p(stream)))
@@ -300,6 +303,12 @@ class PDXIndex:
         return {"bytes": int(out[0]), "clusters_visited": int(out[1]), "merged": int(out[2]),
                 "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])},
                 "cycles_by_phase": {n: int(v) for n, v in zip(["top_level", "start", "rest"], out[9:12])}}
+
+    def kernel_times(self) -> dict:
+        """Durations (ms) of the last search_device(..., time_kernels=True)."""
+        out = np.zeros(3, np.float32)
+        _check(library().pdxg_kernel_times(self._handle().ptr, out))
+        return {"prepare": float(out[0]), "top_level": float(out[1]), "scan": float(out[2])}
 
     def set_pruning_aggressiveness(self, epsilon0: float) -> None:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))

@@ -312,6 +312,8 @@ struct pdxg_index {
     std::vector<uint32_t> rid_cluster, rid_pos;
     cudaStream_t stream = nullptr;
     cudaStream_t stats_stream = nullptr;
+    cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // PDXG_TIME_KERNELS marks
+    bool tev_ready = false, tev_top = false, tev_prep = false;
     Workspace ws;
     std::mutex mu;
     // registered filters (pdxg_filter_register): resident selection bitmaps + passing counts,
@@ -380,6 +382,8 @@ void free_index(pdxg_index* ix) {
     cudaFree(ix->d_rid_pos);
     cudaFree(ix->d_reg_sel);
     cudaFree(ix->d_reg_pass);
+    for (cudaEvent_t e : ix->tev)
+        if (e) cudaEventDestroy(e);
     free_workspace(ix->ws);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
@@ -728,12 +732,21 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     }
     int rc = ensure_ws(ix, w, nq, k);
     if (rc) return rc;
+    const bool timed = (flags & PDXG_TIME_KERNELS) != 0;
+    if (timed) {
+        for (cudaEvent_t& e : ix->tev)
+            if (!e) PDXG_CUDA(cudaEventCreate(&e));
+        ix->tev_ready = false;
+        PDXG_CUDA(cudaEventRecord(ix->tev[0], st));
+    }
     const float* qp = q;
+    ix->tev_prep = !(flags & PDXG_QUERY_TRANSFORMED);
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
         PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, w.d_norms,
                                          w.d_rq, st));
         qp = w.d_rq;
     }
+    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[1], st));
     Launch L;
     rc = plan_search(ix, nq, k, n_order, any_filter, L);
     if (rc) return rc;
@@ -757,8 +770,14 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         rc = run_top_level(ix, w, qp, nq, L, st);
         if (rc) return rc;
     }
+    ix->tev_top = L.p.q_order != nullptr;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
+    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
+    if (timed) {
+        PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
+        ix->tev_ready = true;
+    }
     return PDXG_OK;
 }
 
@@ -1041,6 +1060,23 @@ int pdxg_get_stats(pdxg_index* ix, uint64_t out[12]) {
     unsigned long long h[12];
     PDXG_CUDA(cudaMemcpy(h, ix->ws.d_stats, sizeof(h), cudaMemcpyDeviceToHost));
     for (int i = 0; i < 12; ++i) out[i] = h[i];
+    return PDXG_OK;
+}
+
+int pdxg_kernel_times(pdxg_index* ix, float out[3]) {
+    if (int rc = check_index(ix)) return rc;
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (!ix->tev_ready) return fail(PDXG_ERR_INVALID_ARGUMENT, "no search ran with PDXG_TIME_KERNELS");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    PDXG_CUDA(cudaEventSynchronize(ix->tev[3]));
+    float a = 0.0f, b = 0.0f, c = 0.0f;
+    PDXG_CUDA(cudaEventElapsedTime(&a, ix->tev[0], ix->tev[1]));
+    PDXG_CUDA(cudaEventElapsedTime(&b, ix->tev[1], ix->tev[2]));
+    PDXG_CUDA(cudaEventElapsedTime(&c, ix->tev[2], ix->tev[3]));
+    out[0] = ix->tev_prep ? a : 0.0f;
+    out[1] = ix->tev_top ? b : 0.0f;
+    out[2] = c;
     return PDXG_OK;
 }
 
