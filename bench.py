@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="threads per query CTA (0 = auto)")
     ap.add_argument("--top-mode", type=int, default=None,
                     help="tree top level: 0 auto, 1 per query, 2 batched warp-per-query kernel")
+    ap.add_argument("--rotation-mode", type=int, default=None,
+                    help="0: tcgen05 TF32x3 rotation when available (default), 1: FP32 SIMT GEMM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
     ap.add_argument("--sweep", action="store_true",
@@ -254,6 +256,9 @@ def main():
         ix.set_threads_per_query(args.threads)
     if args.top_mode is not None:
         ix.set_top_level_mode(args.top_mode)
+    if args.rotation_mode is not None:
+        ix.set_rotation_mode(args.rotation_mode)
+    rot_tc = ix.rotation_uses_tensor_cores()
     nq, k, d = cfg["nq"], cfg["k"], cfg["d"]
     Qh = gm.sample(nq, 1 + rank)  # rank-specific batch; the first GT_QUERIES match the GT
     # a dedicated stream: the events below and the engine's launches must share it (handle 0,
@@ -438,6 +443,7 @@ def main():
                 "latency_ms_batch": {"p50": round(float(np.percentile(step_ms, 50)), 3),
                                      "p99": round(float(np.percentile(step_ms, 99)), 3)},
                 "parallelism": f"replicas{world}" if world > 1 else "single",
+                "rotation": "tcgen05 TF32x3" if rot_tc else "FP32 SIMT",
             },
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -453,8 +459,10 @@ def main():
             "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * d * 4,
                     "d2h_bytes_per_step": nq * k * 8 + nq * 4},
-            # per step: [query norms] + rotation + [tree top level] + scan
-            "gpu_launches": args.steps * ((2 if cfg["normalize"] else 1) + (1 if "tree" in cfg["itype"] else 0) + 1),
+            # per step: query preparation (TF32 split + tensor-core GEMM, or [norms] + SIMT GEMM)
+            # + [tree top level] + scan
+            "gpu_launches": args.steps * ((2 if (rot_tc or cfg["normalize"]) else 1)
+                                          + (1 if "tree" in cfg["itype"] else 0) + 1),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -217,6 +217,14 @@ int pdxg_search_requests(pdxg_context* context, const float* queries, uint32_t n
 int pdxg_filter_register(pdxg_index* index, const uint64_t* row_ids, uint64_t n, int32_t* filter_id);
 int pdxg_filter_release(pdxg_index* index, int32_t filter_id);
 
+/* Engine tuning: how queries are rotated (ADSamplingPruner::Rotate, adsampling.hpp:192-246,
+ * an FP32 BLAS sgemm in the reference). 0 = tcgen05 tensor cores with FP32 operands split
+ * into TF32 hi / lo planes (three products, FP32 rounding level) when the device and the
+ * dimension allow it (d >= 512 and a multiple of 4), else the FP32 SIMT GEMM; 1 = always the
+ * FP32 SIMT GEMM. pdxg_rotation_uses_tensor_cores tells which one runs. */
+int pdxg_set_rotation_mode(pdxg_index* index, uint32_t mode);
+int pdxg_rotation_uses_tensor_cores(const pdxg_index* index);
+
 /* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);
 

@@ -74,6 +74,8 @@ def library() -> C.CDLL:
         fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
         fn("pdxg_get_stats", C.c_int, vp, _u64p)
         fn("pdxg_kernel_times", C.c_int, vp, _f32p)
+        fn("pdxg_set_rotation_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_rotation_uses_tensor_cores", C.c_int, vp)
         fn("pdxg_context_create", C.c_int, vp, C.POINTER(vp))
         fn("pdxg_context_free", None, vp)
         fn("pdxg_context_stream", vp, vp)
@@ -316,6 +318,13 @@ class PDXIndex:
     def set_top_level_mode(self, mode: int) -> None:
         """Tree indexes: 0 automatic, 1 top level inside each query's CTA, 2 own launch."""
         _check(library().pdxg_set_top_level_mode(self._handle().ptr, int(mode)))
+
+    def set_rotation_mode(self, mode: int) -> None:
+        """0: tcgen05 TF32x3 rotation when available, 1: FP32 SIMT GEMM."""
+        _check(library().pdxg_set_rotation_mode(self._handle().ptr, int(mode)))
+
+    def rotation_uses_tensor_cores(self) -> bool:
+        return bool(library().pdxg_rotation_uses_tensor_cores(self._handle().ptr))
 
     def set_threads_per_query(self, threads: int) -> None:
         _check(library().pdxg_set_threads_per_query(self._handle().ptr, int(threads)))

@@ -17,6 +17,7 @@
 
 #include "../../include/pdx_b200.h"
 #include "pdxg_common.cuh"
+#include "pdxg_gemm.cuh"
 
 namespace pdxg {
 cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid, cudaStream_t st);
@@ -272,12 +273,17 @@ struct Workspace {
     uint64_t foff_cap = 0;
     uint32_t* d_rows = nullptr;
     uint64_t rows_cap = 0;
+    // tensor-core rotation: TF32 hi / lo planes of the (normalized) queries, GEMM error flag
+    float* d_qhi = nullptr;
+    float* d_qlo = nullptr;
+    uint64_t qhi_cap = 0, qlo_cap = 0;
+    int* d_gemm_err = nullptr;
 };
 
 void free_workspace(Workspace& w) {
     void* ptrs[] = {w.d_q, w.d_rq, w.d_norms, w.d_ids, w.d_dists, w.d_counts, w.d_queue, w.d_order,
                     w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_l1_order,
-                    w.d_l1_count, w.d_req, w.d_foff, w.d_rows};
+                    w.d_l1_count, w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
     for (void* q : ptrs) cudaFree(q);
     w = Workspace();
 }
@@ -300,6 +306,11 @@ struct pdxg_index {
     float* d_cent1 = nullptr;
     float* d_cent0 = nullptr;
     float* d_rot = nullptr;
+    float* d_rot_hi = nullptr;  // M^T split into TF32 hi / lo planes (tensor-core rotation)
+    float* d_rot_lo = nullptr;
+    GemmOperand rot_op{};
+    bool rot_tc = false;        // tensor-core rotation available for this index
+    uint32_t rot_mode = 0;      // 0: tensor cores when available, 1: FP32 SIMT GEMM
     float* d_ratios = nullptr;
     uint32_t* d_rid_cluster = nullptr;  // row id -> cluster (device copy, filters)
     uint32_t* d_rid_pos = nullptr;      // row id -> position in its cluster
@@ -377,6 +388,8 @@ void free_index(pdxg_index* ix) {
     cudaFree(ix->d_cent1);
     cudaFree(ix->d_cent0);
     cudaFree(ix->d_rot);
+    cudaFree(ix->d_rot_hi);
+    cudaFree(ix->d_rot_lo);
     cudaFree(ix->d_ratios);
     cudaFree(ix->d_rid_cluster);
     cudaFree(ix->d_rid_pos);
@@ -537,6 +550,28 @@ int load_from_bytes(const uint8_t* buf, uint64_t size, int device, pdxg_index** 
         upload(ix->d_cent0, ix->l0.centroids, "meso centroids");
     }
     upload(ix->d_rot, ix->rotation, "rotation");
+    // Tensor-core rotation for d >= 512: its error (a fixed number of truncations per K = 32
+    // stage) is below the FP32 SIMT GEMM's (which grows with sqrt(d)) from about that size on;
+    // smaller dimensions keep the SIMT GEMM, the closer match to the reference's sgemm there.
+    if (rc == PDXG_OK && d >= 512 && gemm_available() && gemm_shape_ok(kGemmTF32x3, d)) {
+        // B operand of the tensor-core rotation: M^T (K-major) as TF32 hi / lo planes
+        std::vector<float> th((size_t)d * d), tl((size_t)d * d);
+        for (uint32_t i = 0; i < d; ++i)
+            for (uint32_t j = 0; j < d; ++j) {
+                const float x = ix->rotation[(size_t)i * d + j];
+                uint32_t bits;
+                std::memcpy(&bits, &x, 4);
+                bits &= 0xFFFFE000u;
+                float h;
+                std::memcpy(&h, &bits, 4);
+                th[(size_t)j * d + i] = h;
+                tl[(size_t)j * d + i] = x - h;
+            }
+        upload(ix->d_rot_hi, th, "rotation planes");
+        upload(ix->d_rot_lo, tl, "rotation planes");
+        if (rc == PDXG_OK)
+            ix->rot_tc = make_gemm_operand(ix->rot_op, kGemmTF32x3, ix->d_rot_hi, ix->d_rot_lo, d, d) == 0;
+    }
     if (rc == PDXG_OK) step(cudaMalloc(&ix->d_ratios, sizeof(float) * d), "ratios");
     if (rc == PDXG_OK) rc = upload_ratios(ix);
     if (rc != PDXG_OK) {
@@ -669,6 +704,47 @@ int ensure_ws(pdxg_index* ix, Workspace& w, uint32_t nq, uint32_t k) {
     return PDXG_OK;
 }
 
+// NormalizeQuery + rotation of nq device queries into `out` (ADSamplingPruner::PreprocessQuery,
+// adsampling.hpp:100-113): TF32x3 tensor-core GEMM when available, else the FP32 SIMT GEMM.
+int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float* out, cudaStream_t st) {
+    if (nq == 0) return PDXG_OK;
+    const uint32_t d = ix->d;
+    if (ix->rot_tc && ix->rot_mode == 0) {
+        int rc;
+        if ((rc = dev_grow(w.d_qhi, w.qhi_cap, (uint64_t)nq * d))) return rc;
+        if ((rc = dev_grow(w.d_qlo, w.qlo_cap, (uint64_t)nq * d))) return rc;
+        if (!w.d_gemm_err) {
+            PDXG_CUDA(cudaMalloc(&w.d_gemm_err, sizeof(int)));
+            PDXG_CUDA(cudaMemsetAsync(w.d_gemm_err, 0, sizeof(int), st));
+        }
+        PDXG_CUDA(launch_split_rows(q, nq, d, ix->normalized, w.d_qhi, w.d_qlo, st));
+        GemmOperand a;
+        if (make_gemm_operand(a, kGemmTF32x3, w.d_qhi, w.d_qlo, nq, d) != 0)
+            return fail(PDXG_ERR_CUDA, "cannot encode the query tensor maps");
+        GemmArgs g{};
+        g.M = nq;
+        g.N = d;
+        g.K = d;
+        g.out = out;
+        g.ldo = d;
+        g.error = w.d_gemm_err;
+        PDXG_CUDA(launch_gemm(a, ix->rot_op, kEpiStore, g, st));
+        return PDXG_OK;
+    }
+    PDXG_CUDA(launch_prepare_queries(q, nq, d, ix->d_rot, ix->normalized, w.d_norms, out, st));
+    return PDXG_OK;
+}
+
+// After a synchronization: fails if a tensor-core GEMM of this workspace gave up a wait.
+int check_gemm_error(Workspace& w) {
+    if (!w.d_gemm_err) return PDXG_OK;
+    int h = 0;
+    PDXG_CUDA(cudaMemcpy(&h, w.d_gemm_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h == 0) return PDXG_OK;
+    cudaMemset(w.d_gemm_err, 0, sizeof(int));
+    return fail(PDXG_ERR_CUDA, "tensor-core GEMM gave up waiting (code " + std::to_string(h) + ")");
+}
+
 // Tree top level as its own launch of small CTAs (top_level_kernel): on success the search
 // kernel reads each query's L1 order from L.p.q_order; in the per-query mode the search kernel
 // runs the top level itself.
@@ -742,8 +818,7 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     const float* qp = q;
     ix->tev_prep = !(flags & PDXG_QUERY_TRANSFORMED);
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
-        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, w.d_norms,
-                                         w.d_rq, st));
+        if ((rc = prepare_dev(ix, w, q, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
     }
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[1], st));
@@ -872,7 +947,7 @@ int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t
     PDXG_CUDA(cudaMemcpyAsync(dists, w.d_dists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, st));
     PDXG_CUDA(cudaMemcpyAsync(counts, w.d_counts, sizeof(uint32_t) * nq, cudaMemcpyDeviceToHost, st));
     PDXG_CUDA(cudaStreamSynchronize(st));
-    return PDXG_OK;
+    return check_gemm_error(w);
 }
 
 // Selection bitmap + passing counts of one row-id list (CreatePredicateEvaluator,
@@ -1043,11 +1118,10 @@ int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, floa
     if (rc) return rc;
     cudaStream_t st = ix->stream;
     PDXG_CUDA(cudaMemcpyAsync(ix->ws.d_q, queries, sizeof(float) * nq * ix->d, cudaMemcpyHostToDevice, st));
-    PDXG_CUDA(launch_prepare_queries(ix->ws.d_q, nq, ix->d, ix->d_rot, ix->normalized,
-                                     ix->ws.d_norms, ix->ws.d_rq, st));
+    if ((rc = prepare_dev(ix, ix->ws, ix->ws.d_q, nq, ix->ws.d_rq, st))) return rc;
     PDXG_CUDA(cudaMemcpyAsync(out, ix->ws.d_rq, sizeof(float) * nq * ix->d, cudaMemcpyDeviceToHost, st));
     PDXG_CUDA(cudaStreamSynchronize(st));
-    return PDXG_OK;
+    return check_gemm_error(ix->ws);
 }
 
 int pdxg_get_stats(pdxg_index* ix, uint64_t out[12]) {
@@ -1062,6 +1136,16 @@ int pdxg_get_stats(pdxg_index* ix, uint64_t out[12]) {
     for (int i = 0; i < 12; ++i) out[i] = h[i];
     return PDXG_OK;
 }
+
+int pdxg_set_rotation_mode(pdxg_index* ix, uint32_t mode) {
+    if (int rc = check_index(ix)) return rc;
+    if (mode > 1) return fail(PDXG_ERR_INVALID_ARGUMENT, "rotation mode must be 0 or 1");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    ix->rot_mode = mode;
+    return PDXG_OK;
+}
+
+int pdxg_rotation_uses_tensor_cores(const pdxg_index* ix) { return ix && ix->rot_tc && ix->rot_mode == 0; }
 
 int pdxg_kernel_times(pdxg_index* ix, float out[3]) {
     if (int rc = check_index(ix)) return rc;
@@ -1371,7 +1455,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
     }
     const float* qp = queries;
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
-        PDXG_CUDA(launch_prepare_queries(queries, nq, ix->d, ix->d_rot, ix->normalized, w.d_norms, w.d_rq, st));
+        if ((rc = prepare_dev(ix, w, queries, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
     }
     Launch L;
