@@ -170,10 +170,14 @@ int pdxg_search_device_noalloc(pdxg_index* index, const float* queries, uint32_t
 uint64_t pdxg_noalloc_scratch_bytes(void);
 
 /* Engine tuning, tree indexes: how the top-level (meso-cluster) search of
- * PDXTreeIndex::Search (index.hpp:545-566) runs. 0 = automatic (its own launch when it fits),
- * 1 = inside each query's search CTA, 2 = its own launch of small per-query CTAs that write the
- * L1 visit orders the search kernel then reads (fails with PDXG_ERR_CAPACITY if it cannot run).
- * Results are identical in every mode. */
+ * PDXTreeIndex::Search (index.hpp:545-566) runs. 0 = automatic (the tiled form when the index
+ * and batch fit it, else per-query CTAs), 1 = inside each query's search CTA, 2 = its own
+ * launch of small per-query CTAs, 3 = tiled: a meso probe, exact partial distances per
+ * (meso cluster, query tile) computed once with reuse across queries, and a warp per query
+ * replaying the reference's decisions on them (needs d and the vertical dims to be multiples
+ * of 4 and 16-byte aligned queries). Modes 2 and 3 write the L1 visit orders the search kernel
+ * then reads and fail with PDXG_ERR_CAPACITY if they cannot run. Results are identical in
+ * every mode. */
 int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
 
 /* ---------------------------------------------------------------------------------------

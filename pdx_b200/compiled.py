@@ -316,7 +316,8 @@ class PDXIndex:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))
 
     def set_top_level_mode(self, mode: int) -> None:
-        """Tree indexes: 0 automatic, 1 top level inside each query's CTA, 2 own launch."""
+        """Tree indexes: 0 automatic, 1 top level inside each query's CTA, 2 per-query CTAs,
+        3 tiled (probe, exact partials with reuse across queries, replay)."""
         _check(library().pdxg_set_top_level_mode(self._handle().ptr, int(mode)))
 
     def set_rotation_mode(self, mode: int) -> None:

@@ -90,4 +90,37 @@ struct SearchParams {
     uint32_t order_cap;          // entries of the cluster order list
 };
 
+// Tiled tree top level (pdxg_toplevel.cu): meso probe, per-(meso cluster, query tile) exact
+// partial distances, warp-per-query replay of the top-level PDXearch.
+constexpr int kMaxCheckpoints = 32;
+
+struct TopLevelParams {
+    const uint8_t* arena;
+    DevLevel l0;                 // meso level (F32): its "vectors" are the L1 centroids
+    const float* ratios;         // ADSampling ratio table [d]
+    const float* queries;        // prepared queries [nq x d]
+    uint32_t nq;
+    uint32_t top;                // meso clusters probed per query (row stride of order / off)
+    uint32_t k1;                 // L1 nprobe (row stride of l1_order)
+    const uint32_t* q_nprobe;    // optional per-query L1 nprobe (<= k1)
+    const uint32_t* q_top;       // optional per-query meso probe count (<= top)
+    const int32_t* filter_of;    // optional: queries with filter_of != -1 get no L1 order
+    uint32_t* order;             // [nq x top] probed meso clusters, nearest first
+    uint32_t* off;               // [nq x top] float offset of each probed cluster's partials
+    uint32_t* ntop;              // [nq] meso clusters probed
+    uint32_t* list_count;        // [nL0] queries probing each meso cluster (zeroed before)
+    uint32_t* lists;             // [nL0 x nq] entries q * top + r
+    float* vals;                 // [nq x per_query] partials: ncp checkpoint rows, nb block rows
+    unsigned long long per_query;
+    uint32_t ncp;                // vertical checkpoints (cp[ncp - 1] == dv)
+    uint32_t nvals;              // ncp + n_hblocks rows per probed cluster
+    uint32_t cp[kMaxCheckpoints];
+    uint32_t* l1_order;          // [nq x k1] L1 clusters to visit, nearest first
+    uint32_t* l1_count;          // [nq]
+    unsigned long long* stats;   // optional, SearchParams::stats layout
+    // replay shared memory (bytes per warp and carve-up)
+    uint32_t r_heap_cap, r_work_cap, r_sort_cap, r_pre_floats, r_warp_bytes;
+    uint32_t probe_smem;         // meso probe CTA: query + sort keys
+};
+
 }  // namespace pdxg

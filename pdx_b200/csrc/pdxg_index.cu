@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -26,6 +27,8 @@ cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, cons
                                    bool normalize, float* norms_ws, float* out, cudaStream_t st);
 cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st);
 int top_level_occupancy(size_t smem);
+cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
+                                   cudaStream_t st);
 }  // namespace pdxg
 
 using namespace pdxg;
@@ -254,7 +257,7 @@ struct Workspace {
     // batched tree top level
     uint32_t* d_top_order = nullptr;
     uint64_t top_order_cap = 0;
-    unsigned long long* d_top_off = nullptr;
+    uint32_t* d_top_off = nullptr;
     uint64_t top_off_cap = 0;
     uint32_t* d_top_lists = nullptr;
     uint64_t top_lists_cap = 0;
@@ -282,8 +285,9 @@ struct Workspace {
 
 void free_workspace(Workspace& w) {
     void* ptrs[] = {w.d_q, w.d_rq, w.d_norms, w.d_ids, w.d_dists, w.d_counts, w.d_queue, w.d_order,
-                    w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_l1_order,
-                    w.d_l1_count, w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
+                    w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_top_off,
+                    w.d_top_lists, w.d_top_count, w.d_top_vals, w.d_l1_order, w.d_l1_count,
+                    w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
     for (void* q : ptrs) cudaFree(q);
     w = Workspace();
 }
@@ -317,7 +321,8 @@ struct pdxg_index {
     float eps0 = 1.5f;
     uint32_t nprobe = 0;
     uint32_t threads = 0;
-    uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch
+    uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch of
+                            // per-query CTAs, 3 tiled (probe, partials, replay)
     int num_sms = 0;
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
@@ -745,13 +750,110 @@ int check_gemm_error(Workspace& w) {
     return fail(PDXG_ERR_CUDA, "tensor-core GEMM gave up waiting (code " + std::to_string(h) + ")");
 }
 
-// Tree top level as its own launch of small CTAs (top_level_kernel): on success the search
-// kernel reads each query's L1 order from L.p.q_order; in the per-query mode the search kernel
-// runs the top level itself.
+// Warmup checkpoints of the top-level search: the cumulative DIMENSIONS_FETCHING_SIZES steps
+// from 0, capped at dv (searcher.hpp:374-435, common.hpp:47-49).
+uint32_t warmup_checkpoints(uint32_t dv, uint32_t* cp, uint32_t cap) {
+    static const uint32_t fetch[kNumFetchSizes] = {16, 16, 32, 32, 32, 32, 64, 64, 64, 64,
+                                                   128, 128, 128, 128, 256, 256, 512, 1024, 2048, 16384};
+    uint32_t cur = 0, n = 0;
+    while (cur < dv) {
+        uint32_t last = cur + fetch[n < kNumFetchSizes ? n : kNumFetchSizes - 1];
+        if (last > dv) last = dv;
+        if (n >= cap) return cap + 1;
+        cp[n++] = last;
+        cur = last;
+    }
+    return n;
+}
+
+// Tiled top level (pdxg_toplevel.cu). Returns PDXG_OK with L.p.q_order set when it ran,
+// PDXG_OK with L.p.q_order unset when this index or batch does not fit its limits (the caller
+// then uses the per-query form), or an error.
+int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+    const DevLevel& l0 = L.p.l0;
+    const HostLevel& h0 = ix->l0;
+    if (l0.d % 4 || l0.dv % 4 || l0.dv == 0 || ((uintptr_t)qp & 15) || h0.fc.empty()) return PDXG_OK;
+    TopLevelParams tp{};
+    tp.ncp = warmup_checkpoints(l0.dv, tp.cp, kMaxCheckpoints);
+    if (tp.ncp > (uint32_t)kMaxCheckpoints) return PDXG_OK;
+    const uint32_t k1 = L.p.nprobe, top = L.p.top_nprobe, nL0 = l0.nclusters;
+    if (top == 0 || k1 == 0 || nL0 > 65535 || (uint64_t)nq * top >= (1ull << 32)) return PDXG_OK;
+    tp.nvals = tp.ncp + l0.n_hblocks;
+    // partials of one query: its `top` largest meso clusters at most
+    std::vector<uint32_t> strides(nL0);
+    for (uint32_t i = 0; i < nL0; ++i) strides[i] = (h0.n[i] + 3u) & ~3u;
+    std::sort(strides.begin(), strides.end(), std::greater<uint32_t>());
+    uint64_t per_query = 0;
+    for (uint32_t i = 0; i < std::min(top, nL0); ++i) per_query += (uint64_t)strides[i] * tp.nvals;
+    if (per_query >= (1ull << 31)) return PDXG_OK;
+    const uint64_t vals_bytes = (uint64_t)nq * per_query * 4;
+    if (vals_bytes + (uint64_t)nL0 * nq * 4 > (8ull << 30)) return PDXG_OK;
+    const uint32_t max_n0 = std::max(l0.max_n, 1u);
+    if (max_n0 > (1u << 20)) return PDXG_OK;
+    tp.probe_smem = (uint32_t)(align_up((uint64_t)l0.d * 4, 16) + (uint64_t)next_pow2(nL0) * 8);
+    if (tp.probe_smem + 1024 > ix->max_smem) return PDXG_OK;
+    tp.r_heap_cap = next_pow2(std::max(k1, 2u));
+    tp.r_work_cap = (max_n0 + 31) / 32 * 32;
+    tp.r_sort_cap = std::max({next_pow2(max_n0), tp.r_heap_cap, 2u});
+    tp.r_pre_floats = (uint32_t)((uint64_t)tp.nvals * ((max_n0 + 3) & ~3u));
+    const uint64_t wb = align_up((uint64_t)tp.r_sort_cap * 8 + (uint64_t)tp.r_pre_floats * 4 +
+                                 (uint64_t)tp.r_heap_cap * 8 + (uint64_t)tp.r_work_cap * 8, 16);
+    int warps = 4;
+    while (warps > 1 && (uint64_t)warps * wb + 1024 > ix->max_smem) warps >>= 1;
+    if ((uint64_t)warps * wb + 1024 > ix->max_smem) return PDXG_OK;
+    tp.r_warp_bytes = (uint32_t)wb;
+
+    int rc;
+    if ((rc = dev_grow(w.d_top_order, w.top_order_cap, (uint64_t)nq * top))) return rc;
+    if ((rc = dev_grow(w.d_top_off, w.top_off_cap, (uint64_t)nq * top))) return rc;
+    if ((rc = dev_grow(w.d_top_lists, w.top_lists_cap, (uint64_t)nL0 * nq))) return rc;
+    if ((rc = dev_grow(w.d_top_count, w.top_count_cap, (uint64_t)nL0 + nq))) return rc;
+    if ((rc = dev_grow(w.d_top_vals, w.top_vals_cap, std::max<uint64_t>((uint64_t)nq * per_query, 4)))) return rc;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    tp.arena = ix->arena;
+    tp.l0 = l0;
+    tp.ratios = L.p.ratios;
+    tp.queries = qp;
+    tp.nq = nq;
+    tp.top = top;
+    tp.k1 = k1;
+    tp.q_nprobe = L.p.q_nprobe;
+    tp.q_top = L.p.q_top;
+    tp.filter_of = L.p.filter_of;
+    tp.order = w.d_top_order;
+    tp.off = w.d_top_off;
+    tp.list_count = w.d_top_count;
+    tp.ntop = w.d_top_count + nL0;
+    tp.lists = w.d_top_lists;
+    tp.vals = w.d_top_vals;
+    tp.per_query = per_query;
+    tp.l1_order = w.d_l1_order;
+    tp.l1_count = w.d_l1_count;
+    tp.stats = L.p.stats;
+    const uint32_t vtiles = (max_n0 + 31) / 32;
+    PDXG_CUDA(launch_top_level_tiled(tp, vtiles, warps, st));
+    L.p.q_order = w.d_l1_order;
+    L.p.q_order_count = w.d_l1_count;
+    L.p.q_order_stride = k1;
+    return PDXG_OK;
+}
+
+// Tree top level as its own launch: the tiled form (mode 3, and mode 0 when it fits), else
+// small per-query CTAs (top_level_kernel; mode 2, and mode 0 otherwise). On success the search
+// kernel reads each query's L1 order from L.p.q_order; in mode 1 the search kernel runs the
+// top level itself.
 int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
     if (ix->top_mode == 1) return PDXG_OK;
+    if (ix->top_mode == 0 || ix->top_mode == 3) {
+        int rc = run_top_level_tiled(ix, w, qp, nq, L, st);
+        if (rc || L.p.q_order) return rc;
+        if (ix->top_mode == 3)
+            return fail(PDXG_ERR_CAPACITY, "tiled top level cannot run on this index or batch "
+                                           "(needs d and d_v multiples of 4, 16-byte aligned queries)");
+    }
     SearchParams tp = L.p;
     tp.queries = qp;
     const uint32_t k1 = L.p.nprobe;
@@ -1015,7 +1117,7 @@ int pdxg_set_pruning_aggressiveness(pdxg_index* ix, float eps0) {
 
 int pdxg_set_top_level_mode(pdxg_index* ix, uint32_t mode) {
     if (int rc = check_index(ix)) return rc;
-    if (mode > 2) return fail(PDXG_ERR_INVALID_ARGUMENT, "top-level mode must be 0, 1 or 2");
+    if (mode > 3) return fail(PDXG_ERR_INVALID_ARGUMENT, "top-level mode must be 0, 1, 2 or 3");
     ix->top_mode = mode;
     return PDXG_OK;
 }

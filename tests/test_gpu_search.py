@@ -241,35 +241,78 @@ def test_filtered_edge_cases():
     np.testing.assert_array_equal(a[1], b[1])
 
 
+def _tiled_ok(d):
+    """The tiled top level needs d and the vertical dims to be multiples of 4."""
+    from pdx_b200.layout import dimension_split
+    h, v = dimension_split(d)
+    return d % 4 == 0 and v % 4 == 0
+
+
 @pytest.mark.parametrize("itype", ["pdx_tree_f32", "pdx_tree_u8"])
-@pytest.mark.parametrize("d", [65, 130, 384])
+@pytest.mark.parametrize("d", [65, 130, 384, 512, 1024])
 def test_tree_top_level_modes(port_cls, itype, d):
-    """The batched top level (probe + exact partials + replay) gives the same results as the
-    per-query top level and as the oracle."""
+    """Every form of the top level -- inside the search CTA (1), per-query CTAs (2) and tiled
+    probe + exact partials + replay (3) -- gives the oracle's results."""
     gm = GaussianMixture(d, 20, 0.5, seed=d + 3, unit_norm=True)
     X = gm.sample(4000, 0)
     Q = gm.sample(80, 1)
     f = build_index(X, itype, num_clusters=40, num_meso_clusters=7, normalize=True, seed=3)
+    modes = (1, 2, 3) if _tiled_ok(d) else (1, 2)
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "ix.pdx")
         f.save(p)
         port = port_cls(p)
         ix = compiled.load_index(p)
         R = ix.prepare_queries(Q)
+        if not _tiled_ok(d):
+            ix.set_top_level_mode(3)
+            with pytest.raises(RuntimeError):
+                ix.search_batch(R, 10, transformed=True)
         for nprobe in (0, 3, 12, 39):
             ix.set_nprobe(nprobe)
             port.set_nprobe(nprobe)
             res = {}
-            for mode in (1, 2):
+            for mode in modes:
                 ix.set_top_level_mode(mode)
                 res[mode] = ix.search_batch(R, 10, transformed=True)
             for i in range(len(R)):
                 pi, pd = port.search(R[i], 10, transformed=True)
-                for mode in (1, 2):
+                for mode in modes:
                     ids, ds, cnt = res[mode]
                     assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd,
                                 ctx=f"{itype} d={d} nprobe={nprobe} mode={mode} q{i}")
         port.close()
+
+
+def test_tree_top_level_tiled_stats_match():
+    """The tiled top level replays the per-query search's decisions: the same index bytes and
+    clusters are accounted for as by the per-query kernel."""
+    import torch
+    gm = GaussianMixture(256, 30, 0.4, seed=11, unit_norm=True)
+    X = gm.sample(6000, 0)
+    Q = gm.sample(300, 1)
+    f = build_index(X, "pdx_tree_u8", num_clusters=60, num_meso_clusters=8, normalize=True, seed=5)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        ix = compiled.load_index(p)
+        ix.set_nprobe(10)
+        R = torch.from_numpy(ix.prepare_queries(Q)).cuda()
+        nq, k = len(Q), 10
+        ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+        ds = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+        cnt = torch.empty(nq, dtype=torch.int32, device="cuda")
+        out = {}
+        for mode in (2, 3):
+            ix.set_top_level_mode(mode)
+            ix.search_device(R.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(),
+                             stream=torch.cuda.current_stream().cuda_stream, transformed=True, stats=True)
+            torch.cuda.synchronize()
+            out[mode] = (ix.last_stats(), ids.cpu().numpy().copy(), ds.cpu().numpy().copy())
+        assert out[2][0]["bytes_by_phase"] == out[3][0]["bytes_by_phase"]
+        assert out[2][0]["clusters_visited"] == out[3][0]["clusters_visited"]
+        np.testing.assert_array_equal(out[2][1], out[3][1])
+        np.testing.assert_array_equal(out[2][2], out[3][2])
 
 
 def test_tree_top_level_batched_edge_sizes(port_cls):
@@ -281,13 +324,15 @@ def test_tree_top_level_batched_edge_sizes(port_cls):
             f.save(p)
             port = port_cls(p)
             ix = compiled.load_index(p)
-            ix.set_top_level_mode(2)
             R = ix.prepare_queries(Q)
-            for nprobe, k in ((0, 10), (2, 10), (5, 500)):
-                ix.set_nprobe(nprobe)
-                port.set_nprobe(nprobe)
-                ids, ds, cnt = ix.search_batch(R, k, transformed=True)
-                for i in range(len(R)):
-                    pi, pd = port.search(R[i], k, transformed=True)
-                    assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd, ctx=f"{itype} nprobe={nprobe} k={k} q{i}")
+            for mode in (2, 3):
+                ix.set_top_level_mode(mode)
+                for nprobe, k in ((0, 10), (2, 10), (5, 500)):
+                    ix.set_nprobe(nprobe)
+                    port.set_nprobe(nprobe)
+                    ids, ds, cnt = ix.search_batch(R, k, transformed=True)
+                    for i in range(len(R)):
+                        pi, pd = port.search(R[i], k, transformed=True)
+                        assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd,
+                                    ctx=f"{itype} mode={mode} nprobe={nprobe} k={k} q{i}")
             port.close()
