@@ -136,6 +136,10 @@ int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, f
  * used for the roofline accounting. */
 int pdxg_get_stats(pdxg_index* index, uint64_t out[12]);
 
+/* Engine kernels launched by the last pdxg_search_device call on this index (query
+ * preparation, tree top level and scan; memsets not counted). No counterpart in the reference. */
+uint32_t pdxg_last_launch_count(const pdxg_index* index);
+
 /* Durations (ms) of the last search launched with PDXG_TIME_KERNELS through pdxg_search_device:
  * out[0] query preparation (normalization + rotation), out[1] tree top level, out[2] the scan
  * kernel (0 for a stage that did not run). Waits for that search to finish. No counterpart in

@@ -54,6 +54,7 @@ def library() -> C.CDLL:
         fn("pdxg_set_pruning_aggressiveness", C.c_int, vp, C.c_float)
         fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_top_level_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_last_launch_count", C.c_uint32, vp)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
         fn("pdxg_search_with_order", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u32p, C.c_uint32,
@@ -305,6 +306,10 @@ class PDXIndex:
         return {"bytes": int(out[0]), "clusters_visited": int(out[1]), "merged": int(out[2]),
                 "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])},
                 "cycles_by_phase": {n: int(v) for n, v in zip(["top_level", "start", "rest"], out[9:12])}}
+
+    def last_launch_count(self) -> int:
+        """Engine kernels launched by the last search_device call."""
+        return int(library().pdxg_last_launch_count(self._handle().ptr))
 
     def kernel_times(self) -> dict:
         """Durations (ms) of the last search_device(..., time_kernels=True)."""

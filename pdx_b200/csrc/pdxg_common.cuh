@@ -119,8 +119,9 @@ struct TopLevelParams {
     uint32_t* l1_count;          // [nq]
     unsigned long long* stats;   // optional, SearchParams::stats layout
     // replay shared memory (bytes per warp and carve-up)
-    uint32_t r_heap_cap, r_work_cap, r_sort_cap, r_pre_floats, r_warp_bytes;
-    uint32_t probe_smem;         // meso probe CTA: query + sort keys
+    uint32_t r_heap_cap, r_work_cap, r_sort_cap, r_pre_floats, r_warp_bytes, r_smem;
+    uint32_t probe_smem;         // meso probe CTA: queries + sort keys
+    uint32_t probe_q;            // queries per meso probe CTA (1..8)
 };
 
 }  // namespace pdxg

@@ -330,6 +330,7 @@ struct pdxg_index {
     cudaStream_t stats_stream = nullptr;
     cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // PDXG_TIME_KERNELS marks
     bool tev_ready = false, tev_top = false, tev_prep = false;
+    uint32_t last_launches = 0;  // engine kernels launched by the last search_device_impl
     Workspace ws;
     std::mutex mu;
     // registered filters (pdxg_filter_register): resident selection bitmaps + passing counts,
@@ -617,6 +618,7 @@ struct Launch {
     bool u8 = false;
     int threads = 256;
     int grid = 1;
+    uint32_t top_launches = 0;  // kernels of a separate tree top level
 };
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
@@ -790,17 +792,24 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
     if (vals_bytes + (uint64_t)nL0 * nq * 4 > (8ull << 30)) return PDXG_OK;
     const uint32_t max_n0 = std::max(l0.max_n, 1u);
     if (max_n0 > (1u << 20)) return PDXG_OK;
-    tp.probe_smem = (uint32_t)(align_up((uint64_t)l0.d * 4, 16) + (uint64_t)next_pow2(nL0) * 8);
-    if (tp.probe_smem + 1024 > ix->max_smem) return PDXG_OK;
+    tp.probe_q = 8;
+    auto probe_bytes = [&](uint32_t qn) {
+        return align_up((uint64_t)qn * l0.d * 4, 16) + (uint64_t)qn * next_pow2(nL0) * 8;
+    };
+    while (tp.probe_q > 1 && probe_bytes(tp.probe_q) + 1024 > ix->max_smem) tp.probe_q >>= 1;
+    if (probe_bytes(tp.probe_q) + 1024 > ix->max_smem) return PDXG_OK;
+    tp.probe_smem = (uint32_t)probe_bytes(tp.probe_q);
     tp.r_heap_cap = next_pow2(std::max(k1, 2u));
     tp.r_work_cap = (max_n0 + 31) / 32 * 32;
     tp.r_sort_cap = std::max({next_pow2(max_n0), tp.r_heap_cap, 2u});
     tp.r_pre_floats = (uint32_t)((uint64_t)tp.nvals * ((max_n0 + 3) & ~3u));
-    const uint64_t wb = align_up((uint64_t)tp.r_sort_cap * 8 + (uint64_t)tp.r_pre_floats * 4 +
-                                 (uint64_t)tp.r_heap_cap * 8 + (uint64_t)tp.r_work_cap * 8, 16);
+    const uint64_t wb = align_up((uint64_t)tp.r_sort_cap * 8 + (uint64_t)tp.r_pre_floats * 8 +
+                                 (uint64_t)tp.r_heap_cap * 8 + (uint64_t)tp.r_work_cap * 8 +
+                                 (uint64_t)top * 8, 16);
+    const uint64_t ratio_bytes = align_up((uint64_t)l0.d * 4, 16);
     int warps = 4;
-    while (warps > 1 && (uint64_t)warps * wb + 1024 > ix->max_smem) warps >>= 1;
-    if ((uint64_t)warps * wb + 1024 > ix->max_smem) return PDXG_OK;
+    while (warps > 1 && ratio_bytes + (uint64_t)warps * wb + 1024 > ix->max_smem) warps >>= 1;
+    if (ratio_bytes + (uint64_t)warps * wb + 1024 > ix->max_smem) return PDXG_OK;
     tp.r_warp_bytes = (uint32_t)wb;
 
     int rc;
@@ -832,7 +841,9 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
     tp.l1_count = w.d_l1_count;
     tp.stats = L.p.stats;
     const uint32_t vtiles = (max_n0 + 31) / 32;
+    tp.r_smem = (uint32_t)(ratio_bytes + (uint64_t)warps * wb);
     PDXG_CUDA(launch_top_level_tiled(tp, vtiles, warps, st));
+    L.top_launches = 3;
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
     L.p.q_order_stride = k1;
@@ -892,6 +903,7 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     if (occ <= 0) return fail(PDXG_ERR_CAPACITY, "top-level kernel cannot be resident");
     const int grid = (int)std::min<uint64_t>(nq, (uint64_t)occ * ix->num_sms);
     PDXG_CUDA(launch_top_level(tp, grid, st));
+    L.top_launches = 1;
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
     L.p.q_order_stride = k1;
@@ -919,9 +931,12 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     }
     const float* qp = q;
     ix->tev_prep = !(flags & PDXG_QUERY_TRANSFORMED);
+    uint32_t launches = 1;  // the scan
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
         if ((rc = prepare_dev(ix, w, q, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
+        // TF32 split + tensor-core GEMM, or [norms +] SIMT GEMM
+        launches += (ix->rot_tc && ix->rot_mode == 0) ? 2 : (ix->normalized ? 2 : 1);
     }
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[1], st));
     Launch L;
@@ -946,8 +961,10 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     if (ix->tree && !any_filter && !d_order) {
         rc = run_top_level(ix, w, qp, nq, L, st);
         if (rc) return rc;
+        launches += L.top_launches;
     }
     ix->tev_top = L.p.q_order != nullptr;
+    ix->last_launches = launches;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
@@ -1248,6 +1265,8 @@ int pdxg_set_rotation_mode(pdxg_index* ix, uint32_t mode) {
 }
 
 int pdxg_rotation_uses_tensor_cores(const pdxg_index* ix) { return ix && ix->rot_tc && ix->rot_mode == 0; }
+
+uint32_t pdxg_last_launch_count(const pdxg_index* ix) { return ix ? ix->last_launches : 0; }
 
 int pdxg_kernel_times(pdxg_index* ix, float out[3]) {
     if (int rc = check_index(ix)) return rc;

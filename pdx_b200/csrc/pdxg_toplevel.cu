@@ -36,51 +36,116 @@
 
 namespace pdxg {
 
+__device__ __forceinline__ void warp_sort_u64(uint64_t* a, uint32_t N) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t size = 2; size <= N; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = lane; i < (N >> 1); i += 32) {
+                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
+                const uint32_t hi = lo + stride;
+                const bool asc = (lo & size) == 0;
+                const uint64_t x = a[lo], y = a[hi];
+                if ((x > y) == asc) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // -------------------------------------------------------------------------------- probe
-constexpr int kProbeThreads = 128;
+// CTA = up to kProbeQ queries; thread (centroid c of a group of 32, lane sub of 8) runs lane
+// `sub` of Horizontal (avx2_computers.hpp:47-98: dims sub, sub + 8, ... with FMA) for every
+// query of the CTA, so each centroid element is loaded once per CTA. The 8 lanes then combine
+// in double exactly as horiz_f32_group8 does; the d % 8 tail is added by lane 0 in double.
+constexpr int kProbeThreads = 256;
+constexpr int kProbeQ = 8;
 
 __global__ void __launch_bounds__(kProbeThreads) meso_probe_kernel(const __grid_constant__ TopLevelParams tp) {
     extern __shared__ __align__(16) uint8_t smem[];
     const DevLevel& l0 = tp.l0;
-    const uint32_t q = blockIdx.x;
-    if (tp.filter_of && __ldg(tp.filter_of + q) != -1) {
-        if (threadIdx.x == 0) tp.ntop[q] = 0;
-        return;
-    }
-    const uint32_t d = l0.d, nc = l0.nclusters;
-    float* qf = reinterpret_cast<float*>(smem);
-    uint64_t* keys = reinterpret_cast<uint64_t*>(smem + ((d * 4 + 15) / 16) * 16);
-    const float* src = tp.queries + (size_t)q * d;
-    for (uint32_t i = threadIdx.x; i < d; i += kProbeThreads) qf[i] = __ldg(src + i);
+    const uint32_t d = l0.d, nc = l0.nclusters, qp = tp.probe_q;
+    const uint32_t q0 = blockIdx.x * qp;
+    const uint32_t nqc = (tp.nq - q0) < qp ? (tp.nq - q0) : qp;  // queries of this CTA
+    const uint32_t N = next_pow2(nc);
+    float* qs = reinterpret_cast<float*>(smem);                              // [qp][d]
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem + ((size_t)qp * d * 4 + 15) / 16 * 16);  // [qp][N]
+    for (uint32_t i = threadIdx.x; i < nqc * d; i += kProbeThreads) qs[i] = __ldg(tp.queries + (size_t)q0 * d + i);
     __syncthreads();
     const uint32_t sub = threadIdx.x & 7;
-    for (uint32_t base = 0; base < nc; base += kProbeThreads / 8) {
-        const uint32_t c = base + (threadIdx.x >> 3);
+    const uint32_t full = d & ~7u;
+    for (uint32_t c0 = 0; c0 < nc; c0 += kProbeThreads / 8) {
+        const uint32_t c = c0 + (threadIdx.x >> 3);
         const bool active = c < nc;
-        const float dd = horiz_f32_group8(qf, l0.centroids + (size_t)(active ? c : 0) * d, d, sub, active);
-        if (active && sub == 0) keys[c] = ((uint64_t)__float_as_uint(dd) << 32) | c;
-    }
-    const uint32_t N = next_pow2(nc);
-    for (uint32_t i = nc + threadIdx.x; i < N; i += kProbeThreads) keys[i] = ~0ull;
-    __syncthreads();
-    // the `m` smallest (distance, id) pairs, ascending: the same list as LevelOps::probe
-    block_bitonic_sort<kProbeThreads>(keys, N);
-    const uint32_t topq = tp.q_top ? __ldg(tp.q_top + q) : tp.top;
-    const uint32_t m = topq < nc ? topq : nc;
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (uint32_t r = 0; r < m; ++r) {
-            const uint32_t c = (uint32_t)keys[r];
-            tp.order[(size_t)q * tp.top + r] = c;
-            tp.off[(size_t)q * tp.top + r] = acc;
-            acc += tp.nvals * ((l0.clusters[c].n + 3u) & ~3u);
+        const float* x = l0.centroids + (size_t)(active ? c : 0) * d;
+        float acc[kProbeQ];
+#pragma unroll
+        for (int j = 0; j < kProbeQ; ++j) acc[j] = 0.0f;
+        if (active) {
+            for (uint32_t i = 0; i < full; i += 8) {
+                const float xv = __ldg(x + i + sub);
+#pragma unroll
+                for (int j = 0; j < kProbeQ; ++j) {
+                    if (j < (int)nqc) {
+                        const float t = __fsub_rn(qs[j * d + i + sub], xv);
+                        acc[j] = __fmaf_rn(t, t, acc[j]);
+                    }
+                }
+            }
         }
-        tp.ntop[q] = m;
+#pragma unroll
+        for (int j = 0; j < kProbeQ; ++j) {
+            double sm = (double)acc[j] + (double)__shfl_down_sync(0xffffffffu, acc[j], 4, 8);
+            sm = sm + __shfl_down_sync(0xffffffffu, sm, 2, 8);
+            sm = sm + __shfl_down_sync(0xffffffffu, sm, 1, 8);
+            if (active && sub == 0 && j < (int)nqc) {
+                for (uint32_t i = full; i < d; ++i) {
+                    const float t = __fsub_rn(qs[j * d + i], __ldg(x + i));
+                    sm += (double)__fmul_rn(t, t);
+                }
+                keys[(size_t)j * N + c] = ((uint64_t)__float_as_uint((float)sm) << 32) | c;
+            }
+        }
     }
-    for (uint32_t r = threadIdx.x; r < m; r += kProbeThreads) {
-        const uint32_t c = (uint32_t)keys[r];
-        const uint32_t slot = atomicAdd(tp.list_count + c, 1u);
-        tp.lists[(size_t)c * tp.nq + slot] = q * tp.top + r;
+    for (uint32_t i = threadIdx.x; i < nqc * N; i += kProbeThreads)
+        if (i % N >= nc) keys[i] = ~0ull;
+    __syncthreads();
+    // warp j: query q0 + j -- the `m` smallest (distance, id) pairs, ascending (the list of
+    // LevelOps::probe)
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint32_t j = warp; j < nqc; j += kProbeThreads / 32) {
+        const uint32_t q = q0 + j;
+        if (tp.filter_of && __ldg(tp.filter_of + q) != -1) {
+            if (lane == 0) tp.ntop[q] = 0;
+            continue;
+        }
+        uint64_t* kq = keys + (size_t)j * N;
+        warp_sort_u64(kq, N);
+        const uint32_t topq = tp.q_top ? __ldg(tp.q_top + q) : tp.top;
+        const uint32_t m = topq < nc ? topq : nc;
+        // offsets: exclusive prefix of nvals * stride over the probe list
+        uint32_t carry = 0;
+        for (uint32_t r0 = 0; r0 < m; r0 += 32) {
+            const uint32_t r = r0 + lane;
+            const uint32_t c = r < m ? (uint32_t)kq[r] : 0u;
+            const uint32_t sz = r < m ? tp.nvals * ((l0.clusters[c].n + 3u) & ~3u) : 0u;
+            uint32_t incl = sz;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += t;
+            }
+            if (r < m) {
+                tp.order[(size_t)q * tp.top + r] = c;
+                tp.off[(size_t)q * tp.top + r] = carry + incl - sz;
+                const uint32_t slot = atomicAdd(tp.list_count + c, 1u);
+                tp.lists[(size_t)c * tp.nq + slot] = q * tp.top + r;
+            }
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) tp.ntop[q] = m;
     }
 }
 
@@ -98,6 +163,26 @@ struct PartialsSmem {
     uint32_t qrow[kTQ];           // query index of each slot
     uint32_t cp[kMaxCheckpoints]; // warmup checkpoints
 };
+
+// Packed FP32 pairs (sm_100): each half rounds exactly as the scalar sub.rn / fma.rn.
+__device__ __forceinline__ uint64_t f32x2_dup(float a) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ uint64_t f32x2_sub(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t f32x2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ void f32x2_unpack(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst);
@@ -182,13 +267,11 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
 
     const uint32_t lane = tid & 31, warp = tid >> 5;
     const uint32_t vg = lane & 7, qg = lane >> 3;
-    // thread tile: query slots warp * 16 + qg + 4 i (4 distinct rows per warp and load: distinct
-    // banks) and vectors vg + 8 i, i = 0..3
+    // thread tile: query slots slot0 + 4 i (i = 0..3; 4 consecutive rows per warp and load, so
+    // distinct banks)
     const uint32_t slot0 = warp * 16 + qg;
-    auto store = [&](uint32_t row, uint32_t i, uint32_t b, float val) {
-        const uint32_t sl = slot0 + 4 * i, v = v0 + vg + 8 * b;
-        if (sl < ntile && v < stride) tp.vals[S.qoff[sl] + (size_t)row * stride + v] = val;
-    };
+    auto slot_ok = [&](int i) { return slot0 + 4 * i < ntile; };
+    auto out_row = [&](int i, uint32_t row) { return tp.vals + S.qoff[slot0 + 4 * i] + (size_t)row * stride; };
 
     issue(0);
     cp_async_commit();
@@ -200,13 +283,12 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
         __syncthreads();
     };
 
-    // vertical dims: one chain per (query, vector), stored at every checkpoint
+    // vertical dims: one chain per (query, vector), stored at every checkpoint. Vectors
+    // 2 vg + {0, 1} and 2 vg + 16 + {0, 1}, each adjacent pair in one packed register.
     {
-        float acc[4][4];
+        uint64_t acc[4][2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[i][b] = 0.0f;
+        for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = 0ull;
         uint32_t ck = 0;
         for (uint32_t st = 0; st < nvc; ++st) {
             begin_stage(st);
@@ -217,25 +299,29 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
             for (uint32_t jj = 0; jj < len; jj += 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    float qv[4], xv[4];
+                    uint64_t qv[4], xv[2];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        qv[i] = qs[(slot0 + 4 * i) * kRow + jj + u];
-                        xv[i] = xs[(jj + u) * kTV + vg + 8 * i];
-                    }
+                    for (int i = 0; i < 4; ++i) qv[i] = f32x2_dup(qs[(slot0 + 4 * i) * kRow + jj + u]);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+                        xv[b] = *reinterpret_cast<const uint64_t*>(xs + (jj + u) * kTV + 2 * vg + 16 * b);
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            const float t = __fsub_rn(qv[i], xv[b]);
-                            acc[i][b] = __fmaf_rn(t, t, acc[i][b]);
+                        for (int b = 0; b < 2; ++b) {
+                            const uint64_t t = f32x2_sub(qv[i], xv[b]);
+                            acc[i][b] = f32x2_fma(t, t, acc[i][b]);
                         }
                 }
                 if (ck < ncp && j0 + jj + 4 == S.cp[ck]) {
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) store(ck, i, b, acc[i][b]);
+                        for (int b = 0; b < 2; ++b) {
+                            const uint32_t v = v0 + 2 * vg + 16 * b;
+                            if (slot_ok(i) && v < stride)
+                                *reinterpret_cast<uint64_t*>(out_row(i, ck) + v) = acc[i][b];
+                        }
                     ++ck;
                 }
             }
@@ -243,147 +329,121 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
         }
     }
 
-    // horizontal blocks: per (query, vector) the AVX2 Horizontal sum of each block
+    // horizontal blocks: per (query, vector) the AVX2 Horizontal sum of each block. Lanes
+    // (j, j + 1) of Horizontal run as one packed chain: dims j + 8 t and j + 1 + 8 t are
+    // adjacent in both staged rows.
     for (uint32_t st = nvc; st < nst; ++st) {
         begin_stage(st);
         const float* qs = S.q[st & 1];
         const float* xs = S.x[st & 1];
         const uint32_t row = ncp + (st - nvc);
-        // two passes of 4 queries x 2 vectors keep the double sums in registers
+        // two passes of 4 queries x 2 vectors (vg + 16 h, vg + 16 h + 8)
 #pragma unroll 1
         for (int h = 0; h < 2; ++h) {
             const uint32_t xo0 = (vg + 16 * h) * kRow, xo1 = (vg + 16 * h + 8) * kRow;
-            // lane `sub` of Horizontal: dims sub, sub + 8, ..., sub + 56 with FMA
-            auto chain = [&](int sub, float (&a)[4][2]) {
+            double D0[4][2], D1[4][2], E0[4][2], E1[4][2];
+            // lane pairs in the order they combine: (0,1) + (4,5) -> s0, s1; (2,3) + (6,7) -> s2, s3
+#pragma unroll 1
+            for (int cp2 = 0; cp2 < 4; ++cp2) {
+                const int c = ((cp2 & 1) << 2) | ((cp2 >> 1) << 1);  // 0, 4, 2, 6
+                uint64_t a[4][2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i][0] = a[i][1] = 0.0f;
+                for (int i = 0; i < 4; ++i) a[i][0] = a[i][1] = 0ull;
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
-                    const int dim = sub + 8 * t;
-                    const float x0 = xs[xo0 + dim], x1 = xs[xo1 + dim];
+                    const int dim = c + 8 * t;
+                    const uint64_t x0 = *reinterpret_cast<const uint64_t*>(xs + xo0 + dim);
+                    const uint64_t x1 = *reinterpret_cast<const uint64_t*>(xs + xo1 + dim);
 #pragma unroll
                     for (int i = 0; i < 4; ++i) {
-                        const float qv = qs[(slot0 + 4 * i) * kRow + dim];
-                        float tt = __fsub_rn(qv, x0);
-                        a[i][0] = __fmaf_rn(tt, tt, a[i][0]);
-                        tt = __fsub_rn(qv, x1);
-                        a[i][1] = __fmaf_rn(tt, tt, a[i][1]);
+                        const uint64_t qv = *reinterpret_cast<const uint64_t*>(qs + (slot0 + 4 * i) * kRow + dim);
+                        uint64_t tt = f32x2_sub(qv, x0);
+                        a[i][0] = f32x2_fma(tt, tt, a[i][0]);
+                        tt = f32x2_sub(qv, x1);
+                        a[i][1] = f32x2_fma(tt, tt, a[i][1]);
                     }
                 }
-            };
-            float a[4][2];
-            double D[4][2], E[4][2], F[4][2];
-            // lanes in the order they combine: (0 + 4) + (2 + 6), then (1 + 5) + (3 + 7)
-#pragma unroll 1
-            for (int sp = 0; sp < 8; ++sp) {
-                const int sub = ((sp >> 2) & 1) + ((sp >> 1) & 1) * 2 + (sp & 1) * 4;
-                chain(sub, a);
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
-                        const double av = (double)a[i][b];
-                        if (sp == 0) D[i][b] = av;                                   // lane 0
-                        else if (sp == 1) D[i][b] = D[i][b] + av;                     // s0
-                        else if (sp == 2) E[i][b] = av;                               // lane 2
-                        else if (sp == 3) D[i][b] = D[i][b] + (E[i][b] + av);         // s0 + s2
-                        else if (sp == 4) E[i][b] = av;                               // lane 1
-                        else if (sp == 5) E[i][b] = E[i][b] + av;                     // s1
-                        else if (sp == 6) F[i][b] = av;                               // lane 3
-                        else D[i][b] = D[i][b] + (E[i][b] + (F[i][b] + av));          // + (s1 + s3)
+                        float lo, hi;
+                        f32x2_unpack(a[i][b], lo, hi);
+                        if (cp2 == 0) {          // lanes 0, 1
+                            D0[i][b] = (double)lo;
+                            D1[i][b] = (double)hi;
+                        } else if (cp2 == 1) {   // lanes 4, 5: s0, s1
+                            D0[i][b] = D0[i][b] + (double)lo;
+                            D1[i][b] = D1[i][b] + (double)hi;
+                        } else if (cp2 == 2) {   // lanes 2, 3
+                            E0[i][b] = (double)lo;
+                            E1[i][b] = (double)hi;
+                        } else {                 // lanes 6, 7: s2, s3
+                            E0[i][b] = E0[i][b] + (double)lo;
+                            E1[i][b] = E1[i][b] + (double)hi;
+                        }
                     }
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int b = 0; b < 2; ++b) store(row, i, 2 * h + b, (float)D[i][b]);
+                for (int b = 0; b < 2; ++b) {
+                    const uint32_t v = v0 + vg + 16 * h + 8 * b;
+                    if (slot_ok(i) && v < stride)
+                        out_row(i, row)[v] = (float)((D0[i][b] + E0[i][b]) + (D1[i][b] + E1[i][b]));
+                }
         }
         __syncthreads();
     }
 }
 
 // -------------------------------------------------------------------------------- replay
-__device__ __forceinline__ void warp_sort_u64(uint64_t* a, uint32_t N) {
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t size = 2; size <= N; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t i = lane; i < (N >> 1); i += 32) {
-                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
-                const uint32_t hi = lo + stride;
-                const bool asc = (lo & size) == 0;
-                const uint64_t x = a[lo], y = a[hi];
-                if ((x > y) == asc) {
-                    a[lo] = y;
-                    a[hi] = x;
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
-
-// Largest heap distance and its lowest slot (LevelOps::recompute_top), on every lane.
+// Largest heap distance and its lowest slot (LevelOps::recompute_top), on every lane. The
+// distances are non-negative floats, ordered as their bit patterns.
 __device__ __forceinline__ void warp_heap_top(const float* hd, uint32_t hsize, float& top, uint32_t& slot) {
     const uint32_t lane = threadIdx.x & 31;
-    float best = -1.0f;
-    uint32_t bs = 0xFFFFFFFFu;
+    uint32_t best = 0, bs = 0xFFFFFFFFu;
     for (uint32_t j = lane; j < hsize; j += 32) {
-        const float x = hd[j];
-        if (x > best || (x == best && j < bs)) {
+        const uint32_t x = __float_as_uint(hd[j]);
+        if (bs == 0xFFFFFFFFu || x > best) {
             best = x;
             bs = j;
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const uint32_t os = __shfl_xor_sync(0xffffffffu, bs, o);
-        if (ob > best || (ob == best && os < bs)) {
-            best = ob;
-            bs = os;
-        }
-    }
-    top = best;
-    slot = bs;
+    const uint32_t gmax = __reduce_max_sync(0xffffffffu, best);
+    slot = __reduce_min_sync(0xffffffffu, (best == gmax) ? bs : 0xFFFFFFFFu);
+    top = __uint_as_float(gmax);
 }
 
-// Order-preserving in-place compaction of pos[0, count) to the entries with dist < thr.
-__device__ __forceinline__ uint32_t warp_keep_below(uint32_t* pos, uint32_t count, const float* dist, float thr) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t total = 0;
-    for (uint32_t b0 = 0; b0 < count; b0 += 32) {
-        const uint32_t i = b0 + lane;
-        const bool in = i < count;
-        const uint32_t v = in ? pos[i] : 0u;
-        const bool keep = in && dist[v] < thr;
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        __syncwarp();
-        if (keep) pos[total + __popc(bal & ((1u << lane) - 1u))] = v;
-        total += __popc(bal);
-        __syncwarp();
-    }
-    return total;
-}
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// Shared memory of the replay: the ratio table (d floats) for the CTA, then per warp
+//   sortbuf [r_sort_cap] u64 | pre [2][r_pre_floats] | hd, hid [r_heap_cap] | dist, pos [r_work_cap]
+//   | meta [top] x {cluster, partials offset}
 __global__ void top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const DevLevel& l0 = tp.l0;
+    const uint32_t d = l0.d, dv = l0.dv, nb = l0.n_hblocks, ncp = tp.ncp;
+    float* ratios = reinterpret_cast<float*>(smem);
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) ratios[i] = __ldg(tp.ratios + i);
+    __syncthreads();  // the only block-wide barrier
     const uint32_t q = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (q >= tp.nq) return;  // whole warp; no block-wide barriers below
+    if (q >= tp.nq) return;  // whole warp
     if (tp.filter_of && __ldg(tp.filter_of + q) != -1) {
         if (lane == 0) tp.l1_count[q] = 0;
         return;
     }
-    uint8_t* base = smem + (size_t)warp * tp.r_warp_bytes;
+    uint8_t* base = smem + ((size_t)d * 4 + 15) / 16 * 16 + (size_t)warp * tp.r_warp_bytes;
     uint64_t* sortbuf = reinterpret_cast<uint64_t*>(base);
-    float* pre = reinterpret_cast<float*>(sortbuf + tp.r_sort_cap);
-    float* hd = pre + tp.r_pre_floats;
+    float* prebuf = reinterpret_cast<float*>(sortbuf + tp.r_sort_cap);
+    float* hd = prebuf + 2 * tp.r_pre_floats;
     uint32_t* hid = reinterpret_cast<uint32_t*>(hd + tp.r_heap_cap);
     float* dist = reinterpret_cast<float*>(hid + tp.r_heap_cap);
     uint32_t* pos = reinterpret_cast<uint32_t*>(dist + tp.r_work_cap);
+    uint32_t* meta_c = pos + tp.r_work_cap;   // [top] probed meso cluster
+    uint32_t* meta_o = meta_c + tp.top;       // [top] offset of its partials
 
-    const DevLevel& l0 = tp.l0;
-    const uint32_t d = l0.d, dv = l0.dv, dh = l0.dh, nb = l0.n_hblocks, ncp = tp.ncp;
     const uint32_t k = tp.q_nprobe ? __ldg(tp.q_nprobe + q) : tp.k1;
     const uint32_t m_top = tp.ntop[q];
     const float* qf = tp.queries + (size_t)q * d;
@@ -391,27 +451,50 @@ __global__ void top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
     unsigned long long bytes = (unsigned long long)l0.nclusters * d * 4u;  // centroid probe
     unsigned long long visits = 0;
     auto thr_at = [&](uint32_t cur, float top) {
-        const float r = (cur == d) ? 1.0f : __ldg(tp.ratios + cur);
+        const float r = (cur == d) ? 1.0f : ratios[cur];
         return __fmul_rn(top, r);
+    };
+    for (uint32_t r = lane; r < m_top; r += 32) {
+        meta_c[r] = tp.order[(size_t)q * tp.top + r];
+        meta_o[r] = tp.off[(size_t)q * tp.top + r];
+    }
+    __syncwarp();
+    // next probed cluster with vectors at or after r (m_top if none)
+    auto next_nonempty = [&](uint32_t r) {
+        while (r < m_top && l0.clusters[meta_c[r]].n == 0) ++r;
+        return r;
+    };
+    // all partial rows of probed cluster r into buffer `buf`, asynchronously
+    auto fetch = [&](uint32_t r, int buf) {
+        const uint32_t n = l0.clusters[meta_c[r]].n;
+        const uint32_t n4 = tp.nvals * ((n + 3u) & ~3u) / 4;
+        const float4* src = reinterpret_cast<const float4*>(qvals + meta_o[r]);
+        float* dst = prebuf + (size_t)buf * tp.r_pre_floats;
+        for (uint32_t i = lane; i < n4; i += 32) cp_async16(dst + 4 * i, src + i);
+        cp_async_commit();
     };
 
     uint32_t hsize = 0, slot = 0;
     float top = 0.0f;
-    for (uint32_t r = 0; r < m_top; ++r) {
-        const uint32_t mc = tp.order[(size_t)q * tp.top + r];
-        const DevCluster c = l0.clusters[mc];
+    uint32_t r = next_nonempty(0);
+    int buf = 0;
+    if (r < m_top) fetch(r, 0);
+    while (r < m_top) {
+        const uint32_t rn = next_nonempty(r + 1);
+        if (rn < m_top) {
+            fetch(rn, buf ^ 1);
+            cp_async_wait1();
+        } else {
+            cp_async_wait0();
+        }
+        __syncwarp();
+        const float* pre = prebuf + (size_t)buf * tp.r_pre_floats;
+        const DevCluster c = l0.clusters[meta_c[r]];
         const uint32_t n = c.n;
-        if (n == 0) continue;
         ++visits;
         const uint32_t stride = (n + 3u) & ~3u;
-        // this cluster's partials, all rows at once (one memory round trip)
-        {
-            const float4* src = reinterpret_cast<const float4*>(qvals + tp.off[(size_t)q * tp.top + r]);
-            float4* dst = reinterpret_cast<float4*>(pre);
-            const uint32_t n4 = tp.nvals * stride / 4;
-            for (uint32_t i = lane; i < n4; i += 32) dst[i] = __ldg(src + i);
-            __syncwarp();
-        }
+        // the loop body runs once per non-empty probed cluster; `continue` is not used below
+        do {
         const uint32_t* ids = reinterpret_cast<const uint32_t*>(tp.arena + c.ids_off);
         if (hsize < k) {
             // Start (searcher.hpp:217-281): full distances, push the best k - |heap| in the
@@ -450,9 +533,9 @@ __global__ void top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
             hsize += mm;
             __syncwarp();
             warp_heap_top(hd, hsize, top, slot);
-            continue;
+            break;
         }
-        // Warmup (searcher.hpp:374-435)
+        // Warmup (searcher.hpp:374-435): vertical checkpoints until >= ceil(0.8 n) fail the bound
         const uint32_t needed = (uint32_t)ceilf(__fmul_rn(kSelectivity, (float)n));
         uint32_t cur = 0, step = 0, n_pruned = 0;
         while (n_pruned < needed && cur < dv) {
@@ -466,72 +549,73 @@ __global__ void top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
             cur = last;
             ++step;
         }
-        // Prune (searcher.hpp:437-540)
-        float thr = thr_at(cur, top);
-        uint32_t nsurv = 0;
-        {
-            const float* row = pre + (size_t)(step - 1) * stride;
-            for (uint32_t b0 = 0; b0 < n; b0 += 32) {
-                const uint32_t v = b0 + lane;
-                const float val = v < n ? row[v] : 0.0f;
-                if (v < n) dist[v] = val;
-                const bool keep = v < n && val < thr;
-                const unsigned bal = __ballot_sync(0xffffffffu, keep);
-                if (keep) pos[nsurv + __popc(bal & ((1u << lane) - 1u))] = v;
-                nsurv += __popc(bal);
-            }
-            __syncwarp();
-        }
-        uint32_t cur_v = cur, cur_h = 0;
-        while (dh && nsurv && cur_h < dh) {
-            bytes += (unsigned long long)nsurv * kHDim * 4u;
-            const float* hrow = pre + (size_t)(ncp + cur_h / kHDim) * stride;
-            for (uint32_t i = lane; i < nsurv; i += 32) {
-                const uint32_t v = pos[i];
-                dist[v] = __fadd_rn(dist[v], hrow[v]);
-            }
-            __syncwarp();
-            cur_h += kHDim;
-            cur += kHDim;
-            thr = thr_at(cur, top);
-            nsurv = warp_keep_below(pos, nsurv, dist, thr);
-        }
+        // Prune (searcher.hpp:437-540). The bound's heap top is fixed until the merge, so each
+        // vector's way through the horizontal blocks and the remaining vertical dims depends on
+        // that vector alone: each lane follows its own vectors, and the survivors of every
+        // step are the same, in the same order, as with the step-by-step compaction.
+        const float* erow = pre + (size_t)(step - 1) * stride;
         const float* vert = reinterpret_cast<const float*>(tp.arena + c.vert_off);
-        while (nsurv && cur_v < dv) {
-            const uint32_t last = (cur_v + kHDim < dv) ? cur_v + kHDim : dv;
-            bytes += (unsigned long long)nsurv * (last - cur_v) * 4u;
-            for (uint32_t i = lane; i < nsurv; i += 32) {
-                const uint32_t v = pos[i];
-                float a = dist[v];
+        unsigned long long lane_bytes = 0;
+        for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+            const uint32_t v = c0 + lane;
+            bool alive = v < n;
+            float dd = alive ? erow[v] : 0.0f;
+            uint32_t cv = cur;
+            alive = alive && dd < thr_at(cv, top);
+            for (uint32_t b = 0; alive && b < nb; ++b) {
+                lane_bytes += kHDim * 4u;
+                dd = __fadd_rn(dd, pre[(size_t)(ncp + b) * stride + v]);
+                cv += kHDim;
+                alive = dd < thr_at(cv, top);
+            }
+            uint32_t cur_v = cur;
+            while (alive && cur_v < dv) {
+                const uint32_t last = (cur_v + kHDim < dv) ? cur_v + kHDim : dv;
+                lane_bytes += (unsigned long long)(last - cur_v) * 4u;
                 for (uint32_t j = cur_v; j < last; ++j) {
                     const float t = __fsub_rn(__ldg(qf + j), __ldg(vert + (size_t)j * c.n_pad + v));
-                    a = __fmaf_rn(t, t, a);
+                    dd = __fmaf_rn(t, t, dd);
                 }
-                dist[v] = a;
+                cv = (cv + kHDim < d) ? cv + kHDim : d;
+                cur_v = last;
+                alive = dd < thr_at(cv, top);
+                if (cv == d) break;
             }
-            __syncwarp();
-            cur = (cur + kHDim < d) ? cur + kHDim : d;
-            cur_v = last;
-            thr = thr_at(cur, top);
-            nsurv = warp_keep_below(pos, nsurv, dist, thr);
-            if (cur == d) break;
-        }
-        // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, survivor order
-        for (uint32_t i = 0; i < nsurv; ++i) {
-            const uint32_t v = pos[i];
-            const float dd = dist[v];
-            if (hsize < k || dd < top) {
-                if (lane == 0) {
-                    const uint32_t at = (hsize >= k) ? slot : hsize;
-                    hd[at] = dd;
-                    hid[at] = __ldg(ids + v);
-                }
-                if (hsize < k) ++hsize;
-                __syncwarp();
-                warp_heap_top(hd, hsize, top, slot);
+            if (v < n) {
+                dist[v] = dd;
+                pos[v] = alive ? 1u : 0u;
             }
         }
+        bytes += __reduce_add_sync(0xffffffffu, (uint32_t)lane_bytes);
         __syncwarp();
+        // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, in position order
+        for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+            const uint32_t v = c0 + lane;
+            const bool alive = v < n && pos[v] != 0u;
+            const float dd = alive ? dist[v] : 0.0f;
+            const uint32_t idv = alive ? __ldg(ids + v) : 0u;
+            unsigned bal = __ballot_sync(0xffffffffu, alive);
+            while (bal) {
+                const int i = __ffs(bal) - 1;
+                bal &= bal - 1;
+                const float ddi = __shfl_sync(0xffffffffu, dd, i);
+                const uint32_t idi = __shfl_sync(0xffffffffu, idv, i);
+                if (hsize < k || ddi < top) {
+                    if (lane == 0) {
+                        const uint32_t at = (hsize >= k) ? slot : hsize;
+                        hd[at] = ddi;
+                        hid[at] = idi;
+                    }
+                    if (hsize < k) ++hsize;
+                    __syncwarp();
+                    warp_heap_top(hd, hsize, top, slot);
+                }
+            }
+        }
+        } while (false);
+        __syncwarp();  // every lane is done with `pre` before the next fetch overwrites it
+        r = rn;
+        buf ^= 1;
     }
     // BuildResultSetFromHeap (searcher.hpp:568-585): the L1 clusters, nearest first
     const uint32_t N = next_pow2(hsize ? hsize : 1);
@@ -562,7 +646,7 @@ cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, in
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(meso_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tp.probe_smem);
     if (e != cudaSuccess) return e;
-    meso_probe_kernel<<<tp.nq, kProbeThreads, tp.probe_smem, st>>>(tp);
+    meso_probe_kernel<<<(tp.nq + tp.probe_q - 1) / tp.probe_q, kProbeThreads, tp.probe_smem, st>>>(tp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int psmem = (int)sizeof(PartialsSmem);
     e = cudaFuncSetAttribute(meso_partials_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem);
@@ -570,7 +654,7 @@ cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, in
     dim3 grid((tp.nq + kTQ - 1) / kTQ, tp.l0.nclusters, vtiles);
     meso_partials_kernel<<<grid, kPartialsThreads, psmem, st>>>(tp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const size_t rsmem = (size_t)tp.r_warp_bytes * replay_warps;
+    const size_t rsmem = tp.r_smem;
     e = cudaFuncSetAttribute(top_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem);
     if (e != cudaSuccess) return e;
     top_replay_kernel<<<(tp.nq + replay_warps - 1) / replay_warps, 32 * replay_warps, rsmem, st>>>(tp);
