@@ -184,6 +184,13 @@ uint64_t pdxg_noalloc_scratch_bytes(void);
  * every mode. */
 int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
 
+/* Engine tuning, U8 tree indexes: the Start of PDXearch (searcher.hpp:217-281) on each query's
+ * first visited cluster. 0 = batched when the batch has at least 32 queries and the L1 visit
+ * orders come from a separate top level: queries are grouped by first cluster and the exact
+ * distances computed once per cluster and group, ahead of the scan; 1 = inside each query's
+ * scan CTA. Results are identical in both modes. No counterpart in the reference. */
+int pdxg_set_start_mode(pdxg_index* index, uint32_t mode);
+
 /* ---------------------------------------------------------------------------------------
  * Serving-style batches. A context owns a workspace and a CUDA stream; work issued on
  * different contexts of one index runs concurrently. No counterpart in the reference (one
@@ -233,7 +240,7 @@ int pdxg_filter_release(pdxg_index* index, int32_t filter_id);
 int pdxg_set_rotation_mode(pdxg_index* index, uint32_t mode);
 int pdxg_rotation_uses_tensor_cores(const pdxg_index* index);
 
-/* Engine tuning: threads per query CTA (128, 256 or 512; 0 = automatic). */
+/* Engine tuning: threads per query CTA (64, 128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);
 
 #ifdef __cplusplus

@@ -55,6 +55,7 @@ def library() -> C.CDLL:
         fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_top_level_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_last_launch_count", C.c_uint32, vp)
+        fn("pdxg_set_start_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
         fn("pdxg_search_with_order", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u32p, C.c_uint32,
@@ -324,6 +325,10 @@ class PDXIndex:
         """Tree indexes: 0 automatic, 1 top level inside each query's CTA, 2 per-query CTAs,
         3 tiled (probe, exact partials with reuse across queries, replay)."""
         _check(library().pdxg_set_top_level_mode(self._handle().ptr, int(mode)))
+
+    def set_start_mode(self, mode: int) -> None:
+        """U8 tree indexes: 0 batched first-cluster Start when it fits, 1 inside the scan."""
+        _check(library().pdxg_set_start_mode(self._handle().ptr, int(mode)))
 
     def set_rotation_mode(self, mode: int) -> None:
         """0: tcgen05 TF32x3 rotation when available, 1: FP32 SIMT GEMM."""

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "pdxg_common.cuh"
+
 namespace pdxg {
 
 struct Scalars {
@@ -190,6 +192,33 @@ __device__ __forceinline__ float horiz_f32_group8(const float* q, const float* x
         }
     }
     return (float)s;
+}
+
+// QuantizeEmbedding (scalar.hpp:76-94) of one packed 32-bit word of a U8 level's query: words
+// [0, qw_hoff) hold the vertical dims 4 w .. 4 w + 3 (zero past d_v), words from qw_hoff the
+// horizontal dims in 64-dim blocks.
+__device__ __forceinline__ uint32_t quantize_word(const float* qf, const DevLevel& lv, uint32_t w) {
+    uint32_t word = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        uint32_t dim;
+        bool valid;
+        if (w < lv.qw_hoff) {
+            dim = w * 4 + b;
+            valid = dim < lv.dv;
+        } else {
+            dim = lv.dv + (w - lv.qw_hoff) * 4 + b;
+            valid = true;
+        }
+        uint32_t byte = 0;
+        if (valid) {
+            const float v = __fmul_rn(__fsub_rn(qf[dim], lv.base), lv.scale);
+            const int r = (int)roundf(v);
+            byte = r > 255 ? 255u : (r < 0 ? 0u : (uint32_t)r);
+        }
+        word |= byte << (8 * b);
+    }
+    return word;
 }
 
 }  // namespace pdxg

@@ -83,8 +83,15 @@ struct SearchParams {
     const uint32_t* q_order;        // [nq x q_order_stride]
     const uint32_t* q_order_count;  // [nq]
     uint32_t q_order_stride;
+    // batched Start (pdxg_start.cu): exact U8 distances to every vector of each query's first
+    // visited cluster, computed ahead with reuse across queries
+    const int32_t* start_row;       // optional [nq]: row in start_dist, -1 = none
+    const uint32_t* start_first;    // [nq] the cluster of that row
+    const uint32_t* start_dist;     // [rows x start_stride]
+    uint32_t start_stride;
     // shared-memory carve-up (bytes), computed by the host
-    uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_total;
+    uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_bits, smem_total;
+    uint32_t bits_cap;           // words of the survivor bitmap (work_cap / 32); the prefix follows
     uint32_t work_cap;           // entries of the dist / pos work arrays (multiple of 32, >= heap_cap)
     uint32_t heap_cap;           // entries of the heap arrays (power of two)
     uint32_t order_cap;          // entries of the cluster order list
@@ -122,6 +129,30 @@ struct TopLevelParams {
     uint32_t r_heap_cap, r_work_cap, r_sort_cap, r_pre_floats, r_warp_bytes, r_smem;
     uint32_t probe_smem;         // meso probe CTA: queries + sort keys
     uint32_t probe_q;            // queries per meso probe CTA (1..8)
+};
+
+// Batched Start (pdxg_start.cu).
+struct StartParams {
+    const uint8_t* arena;
+    DevLevel l1;
+    const float* queries;         // prepared queries [nq x d]
+    uint32_t nq;
+    const uint32_t* q_order;      // [nq x q_order_stride] each query's L1 visit order
+    const uint32_t* q_order_count;
+    uint32_t q_order_stride;
+    const int32_t* filter_of;     // optional: queries with filter_of != -1 are left out
+    uint32_t* cl_count;           // [n1] queries per first cluster (zeroed before)
+    uint32_t* cl_off;             // [n1] first row of each cluster
+    uint32_t* cl_items;           // [n1] first work item of each cluster
+    uint32_t* first_cl;           // [nq] first non-empty visited cluster (~0u: none)
+    uint32_t* slot_of;            // [nq] position among that cluster's queries
+    int32_t* row_of;              // [nq] row in dist (-1: none)
+    uint32_t* sorted_q;           // [nq] queries grouped by first cluster (row order)
+    uint32_t* items;              // [2 x item bound] (cluster, query chunk << 16 | vector chunk)
+    uint32_t* n_items;            // [1]
+    uint32_t* queue;              // [1] work counter
+    uint32_t* dist;               // [nq x stride] exact U8 distances
+    uint32_t stride;              // >= largest L1 cluster
 };
 
 }  // namespace pdxg

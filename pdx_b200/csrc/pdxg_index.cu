@@ -29,6 +29,10 @@ cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st);
 int top_level_occupancy(size_t smem);
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
                                    cudaStream_t st);
+cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t st);
+int start_dist_occupancy(size_t smem);
+size_t start_dist_smem(const DevLevel& lv);
+uint64_t start_item_bound(uint32_t nq, uint32_t n1, uint32_t max_n);
 }  // namespace pdxg
 
 using namespace pdxg;
@@ -269,6 +273,16 @@ struct Workspace {
     uint64_t l1_order_cap = 0;
     uint32_t* d_l1_count = nullptr;
     uint64_t l1_count_cap = 0;
+    // batched Start: per-cluster counters ([3 x n1]), per-query arrays ([4 x nq]), work items,
+    // counters, distances
+    uint32_t* d_st_cl = nullptr;
+    uint64_t st_cl_cap = 0;
+    uint32_t* d_st_q = nullptr;
+    uint64_t st_q_cap = 0;
+    uint32_t* d_st_items = nullptr;
+    uint64_t st_items_cap = 0;
+    uint32_t* d_st_dist = nullptr;
+    uint64_t st_dist_cap = 0;
     // per-query request parameters (pdxg_search_requests)
     uint32_t* d_req = nullptr;  // q_k | q_nprobe | q_top | filter_of, nq each
     uint64_t req_cap = 0;
@@ -287,6 +301,7 @@ void free_workspace(Workspace& w) {
     void* ptrs[] = {w.d_q, w.d_rq, w.d_norms, w.d_ids, w.d_dists, w.d_counts, w.d_queue, w.d_order,
                     w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_top_off,
                     w.d_top_lists, w.d_top_count, w.d_top_vals, w.d_l1_order, w.d_l1_count,
+                    w.d_st_cl, w.d_st_q, w.d_st_items, w.d_st_dist,
                     w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
     for (void* q : ptrs) cudaFree(q);
     w = Workspace();
@@ -323,6 +338,7 @@ struct pdxg_index {
     uint32_t threads = 0;
     uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch of
                             // per-query CTAs, 3 tiled (probe, partials, replay)
+    uint32_t start_mode = 0;  // U8 first-cluster Start: 0 batched when it fits, 1 in the scan
     int num_sms = 0;
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
@@ -619,6 +635,7 @@ struct Launch {
     int threads = 256;
     int grid = 1;
     uint32_t top_launches = 0;  // kernels of a separate tree top level
+    uint32_t start_launches = 0;  // kernels of the batched Start
 };
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
@@ -667,6 +684,9 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
     off += heap_cap * 8;
     p.smem_order = off;
     off += (uint32_t)align_up((uint64_t)order_cap * 4, 16);
+    p.smem_bits = off;
+    p.bits_cap = work_cap / 32;
+    off += (uint32_t)align_up((uint64_t)p.bits_cap * 8, 16);
     p.smem_total = off;
     p.work_cap = work_cap;
     p.heap_cap = heap_cap;
@@ -676,7 +696,7 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
                                            " B) exceeds the device limit; cluster, k or nprobe too large");
     L.u8 = ix->u8;
     int threads = (int)ix->threads;
-    if (threads == 0) threads = 256;
+    if (threads == 0) threads = 128;  // measured fastest on B200 (IVF2 SQ8 1M x 1024)
     L.threads = threads;
     const int occ = search_occupancy(L.u8, threads, off);
     if (occ <= 0) return fail(PDXG_ERR_CAPACITY, "search kernel cannot be resident with this configuration");
@@ -883,6 +903,9 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     off += heap_cap * 8;
     tp.smem_order = off;
     off += (uint32_t)align_up((uint64_t)std::max(top, 1u) * 4, 16);
+    tp.smem_bits = off;
+    tp.bits_cap = work_cap / 32;
+    off += (uint32_t)align_up((uint64_t)tp.bits_cap * 8, 16);
     tp.smem_total = off;
     tp.work_cap = work_cap;
     tp.heap_cap = heap_cap;
@@ -907,6 +930,57 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
     L.p.q_order_stride = k1;
+    return PDXG_OK;
+}
+
+// Batched Start (pdxg_start.cu) for U8 levels whose visit orders are known before the scan
+// (tree indexes with a separate top level). Sets L.p.start_* when it ran; a batch outside its
+// limits leaves them unset and the scan runs Start itself.
+constexpr uint32_t kStartMinQueries = 32;
+
+int run_start_batched(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+    L.p.start_row = nullptr;
+    if (!ix->u8 || !L.p.q_order || ix->start_mode == 1 || nq < kStartMinQueries) return PDXG_OK;
+    const uint32_t n1 = L.p.l1.nclusters;
+    const uint32_t stride = (std::max(L.p.l1.max_n, 1u) + 3) & ~3u;
+    const uint64_t items = start_item_bound(nq, n1, std::max(L.p.l1.max_n, 1u));
+    if ((uint64_t)nq * stride * 4 > (4ull << 30) || items > 0xFFFFFFFFull || nq > (1u << 20)) return PDXG_OK;
+    const size_t smem = start_dist_smem(L.p.l1);
+    if (smem + 1024 > ix->max_smem) return PDXG_OK;
+    const int occ = start_dist_occupancy(smem);
+    if (occ <= 0) return PDXG_OK;
+    int rc;
+    if ((rc = dev_grow(w.d_st_cl, w.st_cl_cap, (uint64_t)3 * n1))) return rc;
+    if ((rc = dev_grow(w.d_st_q, w.st_q_cap, (uint64_t)4 * nq + 2))) return rc;
+    if ((rc = dev_grow(w.d_st_items, w.st_items_cap, 2 * items))) return rc;
+    if ((rc = dev_grow(w.d_st_dist, w.st_dist_cap, (uint64_t)nq * stride))) return rc;
+    StartParams sp{};
+    sp.arena = ix->arena;
+    sp.l1 = L.p.l1;
+    sp.queries = qp;
+    sp.nq = nq;
+    sp.q_order = L.p.q_order;
+    sp.q_order_count = L.p.q_order_count;
+    sp.q_order_stride = L.p.q_order_stride;
+    sp.filter_of = L.p.filter_of;
+    sp.cl_count = w.d_st_cl;
+    sp.cl_off = w.d_st_cl + n1;
+    sp.cl_items = w.d_st_cl + 2 * (uint64_t)n1;
+    sp.first_cl = w.d_st_q;
+    sp.slot_of = w.d_st_q + nq;
+    sp.row_of = reinterpret_cast<int32_t*>(w.d_st_q + 2 * (uint64_t)nq);
+    sp.sorted_q = w.d_st_q + 3 * (uint64_t)nq;
+    sp.n_items = w.d_st_q + 4 * (uint64_t)nq;
+    sp.queue = w.d_st_q + 4 * (uint64_t)nq + 1;
+    sp.items = w.d_st_items;
+    sp.dist = w.d_st_dist;
+    sp.stride = stride;
+    PDXG_CUDA(launch_start_batched(sp, occ * ix->num_sms, st));
+    L.p.start_row = sp.row_of;
+    L.p.start_first = sp.first_cl;
+    L.p.start_dist = sp.dist;
+    L.p.start_stride = stride;
+    L.start_launches = 3;
     return PDXG_OK;
 }
 
@@ -964,9 +1038,12 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         launches += L.top_launches;
     }
     ix->tev_top = L.p.q_order != nullptr;
+    // the batched Start belongs to the scan's time
+    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
+    if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
+    launches += L.start_launches;
     ix->last_launches = launches;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
-    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     if (timed) {
         PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
@@ -1139,10 +1216,17 @@ int pdxg_set_top_level_mode(pdxg_index* ix, uint32_t mode) {
     return PDXG_OK;
 }
 
+int pdxg_set_start_mode(pdxg_index* ix, uint32_t mode) {
+    if (int rc = check_index(ix)) return rc;
+    if (mode > 1) return fail(PDXG_ERR_INVALID_ARGUMENT, "start mode must be 0 or 1");
+    ix->start_mode = mode;
+    return PDXG_OK;
+}
+
 int pdxg_set_threads_per_query(pdxg_index* ix, uint32_t threads) {
     if (int rc = check_index(ix)) return rc;
-    if (threads != 0 && threads != 128 && threads != 256 && threads != 512)
-        return fail(PDXG_ERR_INVALID_ARGUMENT, "threads per query must be 0, 128, 256 or 512");
+    if (threads != 0 && threads != 64 && threads != 128 && threads != 256 && threads != 512)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "threads per query must be 0, 64, 128, 256 or 512");
     ix->threads = threads;
     return PDXG_OK;
 }
@@ -1598,6 +1682,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
     L.p.queue = w.d_queue;
     if (ix->tree && any_plain) {
         if ((rc = run_top_level(ix, w, qp, nq, L, st))) return rc;
+        if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
     }
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));

@@ -42,6 +42,7 @@ struct Shared {
     float* hd;          // [heap_cap] heap distances
     uint32_t* hid;      // [heap_cap] heap row ids
     uint32_t* order;    // [order_cap] cluster visit order
+    uint32_t* bits;     // [bits_cap] survivor bitmap of the last warmup step, then its prefix
     uint64_t* sortw;    // work region viewed as u64 [work_cap]
     uint64_t* sorth;    // heap region viewed as u64 [heap_cap]
 };
@@ -69,6 +70,8 @@ struct LevelOps {
     const uint32_t* fsel;   // this query's selection bitmap over the level (null = unfiltered)
     const uint32_t* fpass;  // this query's passing count per cluster
     bool top_level;         // the tree's meso-cluster search
+    int32_t pre_row = -1;   // row of this query's batched first-cluster distances (U8), or -1
+    uint32_t pre_cluster = 0xFFFFFFFFu;  // the cluster they belong to
 
     __device__ LevelOps(const SearchParams& p_, const DevLevel& lv_, Shared& sh_, Scalars& s_,
                         int filter, bool top_level_ = false)
@@ -122,26 +125,32 @@ struct LevelOps {
     }
 
     // Vertical dims [d0, d1) for all vectors; returns #vectors with dist >= thr (counted only
-    // when count is set). For U8, d0 is a multiple of 4; a trailing partial group is reached
-    // only with d1 == dv and its padding bytes are zero in both query and data.
+    // when count is set, and then sh.bits receives the bitmap of the vectors below thr, one
+    // word per 32 positions). Distances start from 0 with from_zero, else from sh.dist. For U8,
+    // d0 is a multiple of 4; a trailing partial group is reached only with d1 == dv and its
+    // padding bytes are zero in both query and data.
     // Each thread keeps kVPT vectors (v, v + T, ...) and issues a whole batch of rows for all of
     // them before consuming any, so one step costs one memory round trip, not one per vector.
+    // The loop runs per warp (base is warp-uniform), so every lane reaches each ballot.
     static constexpr int kVPT = 4;
     __device__ uint32_t vertical_all(const DevCluster& c, uint32_t d0, uint32_t d1, bool count,
-                                     uint32_t thr) {
+                                     uint32_t thr, bool from_zero = false) {
         const uint32_t* base = vert(c);
         const uint32_t n = c.n, np = c.n_pad;
+        const uint32_t lane = lane_id();
         uint32_t pruned = 0;
-        for (uint32_t v0 = threadIdx.x; v0 < n; v0 += T * kVPT) {
+        for (uint32_t wb = threadIdx.x - lane; wb < n; wb += T * kVPT) {
+            const uint32_t v0 = wb + lane;
             bool act[kVPT];
 #pragma unroll
             for (int k = 0; k < kVPT; ++k) act[k] = v0 + k * T < n;
+            bool keep[kVPT];
             if constexpr (U8) {
-                constexpr int GB = 8;  // groups per batch
+                constexpr int GB = 4;  // groups per batch
                 const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
                 uint32_t acc[kVPT];
 #pragma unroll
-                for (int k = 0; k < kVPT; ++k) acc[k] = act[k] ? sh.dist[v0 + k * T] : 0u;
+                for (int k = 0; k < kVPT; ++k) acc[k] = (act[k] && !from_zero) ? sh.dist[v0 + k * T] : 0u;
                 for (uint32_t g = g0; g < g1; g += GB) {
                     uint32_t x[kVPT][GB];
 #pragma unroll
@@ -160,6 +169,7 @@ struct LevelOps {
                 }
 #pragma unroll
                 for (int k = 0; k < kVPT; ++k) {
+                    keep[k] = act[k] && acc[k] < thr;
                     if (act[k]) {
                         sh.dist[v0 + k * T] = acc[k];
                         pruned += (count && acc[k] >= thr) ? 1u : 0u;
@@ -170,7 +180,7 @@ struct LevelOps {
                 const float* fb = reinterpret_cast<const float*>(base);
                 float acc[kVPT];
 #pragma unroll
-                for (int k = 0; k < kVPT; ++k) acc[k] = act[k] ? __uint_as_float(sh.dist[v0 + k * T]) : 0.0f;
+                for (int k = 0; k < kVPT; ++k) acc[k] = (act[k] && !from_zero) ? __uint_as_float(sh.dist[v0 + k * T]) : 0.0f;
                 for (uint32_t j = d0; j < d1; j += DB) {
                     float x[kVPT][DB];
 #pragma unroll
@@ -190,16 +200,61 @@ struct LevelOps {
                         }
                     }
                 }
+                const float tf = __uint_as_float(thr);
 #pragma unroll
                 for (int k = 0; k < kVPT; ++k) {
+                    keep[k] = act[k] && acc[k] < tf;
                     if (act[k]) {
                         sh.dist[v0 + k * T] = __float_as_uint(acc[k]);
-                        pruned += (count && acc[k] >= __uint_as_float(thr)) ? 1u : 0u;
+                        pruned += (count && acc[k] >= tf) ? 1u : 0u;
                     }
+                }
+            }
+            if (count) {
+#pragma unroll
+                for (int k = 0; k < kVPT; ++k) {
+                    const unsigned m = __ballot_sync(0xffffffffu, keep[k]);
+                    if (lane == 0 && wb + k * T < n) sh.bits[(wb + k * T) >> 5] = m;
                 }
             }
         }
         return count ? block_sum<T>(pruned, s) : 0u;
+    }
+
+    // Positions of the set bits of sh.bits over [0, n), ascending, into sh.pos; returns their
+    // number. sh.bits must be complete (a barrier after it was written).
+    __device__ uint32_t compact_bits(uint32_t n) {
+        const uint32_t words = (n + 31) >> 5;
+        uint32_t* pref = sh.bits + p.bits_cap;
+        if (threadIdx.x < 32) {
+            const uint32_t lane = lane_id();
+            uint32_t carry = 0;
+            for (uint32_t w0 = 0; w0 < words; w0 += 32) {
+                const uint32_t w = w0 + lane;
+                const uint32_t cnt = w < words ? __popc(sh.bits[w]) : 0u;
+                uint32_t incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (uint32_t)o) incl += t;
+                }
+                if (w < words) pref[w] = carry + incl - cnt;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) s.sc[2] = carry;
+        }
+        __syncthreads();
+        for (uint32_t w = threadIdx.x; w < words; w += T) {
+            uint32_t b = sh.bits[w], at = pref[w];
+            while (b) {
+                const uint32_t i = __ffs(b) - 1;
+                b &= b - 1;
+                sh.pos[at++] = w * 32 + i;
+            }
+        }
+        const uint32_t total = s.sc[2];
+        __syncthreads();
+        return total;
     }
 
     // Vertical dims [d0, d1) for the first npos listed positions (gathered access).
@@ -314,29 +369,30 @@ struct LevelOps {
         __syncthreads();
     }
 
+    // Largest heap distance and its lowest slot, on every lane of the calling warp. Heap
+    // distances are non-negative floats, ordered as their bit patterns.
+    __device__ __forceinline__ void warp_heap_top(uint32_t hsize, float& top, uint32_t& slot) const {
+        const uint32_t lane = lane_id();
+        uint32_t best = 0, bs = 0xFFFFFFFFu;
+        for (uint32_t i = lane; i < hsize; i += 32) {
+            const uint32_t x = __float_as_uint(sh.hd[i]);
+            if (bs == 0xFFFFFFFFu || x > best) {
+                best = x;
+                bs = i;
+            }
+        }
+        const uint32_t gmax = __reduce_max_sync(0xffffffffu, best);
+        slot = __reduce_min_sync(0xffffffffu, best == gmax ? bs : 0xFFFFFFFFu);
+        top = __uint_as_float(gmax);
+    }
+
     __device__ void recompute_top() {
         if (threadIdx.x < 32) {
-            const uint32_t lane = lane_id();
-            float best = -1.0f;
-            uint32_t slot = 0xFFFFFFFFu;
-            for (uint32_t i = lane; i < s.hsize; i += 32) {
-                const float v = sh.hd[i];
-                if (v > best || (v == best && i < slot)) {
-                    best = v;
-                    slot = i;
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-                const uint32_t os = __shfl_xor_sync(0xffffffffu, slot, off);
-                if (ob > best || (ob == best && os < slot)) {
-                    best = ob;
-                    slot = os;
-                }
-            }
-            if (lane == 0) {
-                s.top = best;
+            float top;
+            uint32_t slot;
+            warp_heap_top(s.hsize, top, slot);
+            if (threadIdx.x == 0) {
+                s.top = top;
                 s.top_slot = slot;
             }
         }
@@ -384,6 +440,18 @@ struct LevelOps {
         push_smallest(c, m);
     }
 
+    // searcher.hpp:217-281 on distances computed ahead by the batched Start (pdxg_start.cu):
+    // the same exact U8 sums, read instead of recomputed.
+    __device__ void start_pre(const DevCluster& c, uint32_t k) {
+        count_bytes((unsigned long long)c.n * lv.d * kElem, kStart);
+        const uint32_t* src = p.start_dist + (size_t)pre_row * p.start_stride;
+        for (uint32_t v = threadIdx.x; v < c.n; v += T) sh.dist[v] = __ldg(src + v);
+        __syncthreads();
+        uint32_t m = k - s.hsize;
+        if (m > c.n) m = c.n;
+        push_smallest(c, m);
+    }
+
     // searcher.hpp:283-372
     __device__ void filtered_start(const DevCluster& c, uint32_t k, uint32_t passing) {
         zero_dist(c.n);
@@ -414,9 +482,9 @@ struct LevelOps {
     __device__ void prune_cluster(const DevCluster& c, uint32_t k, uint32_t passing) {
         const uint32_t n = c.n;
         uint32_t cur = 0;
-        zero_dist(n);
         bool skip_warmup = false;
         if (fsel) {
+            zero_dist(n);
             const uint32_t mask = mask_raw();
             for (uint32_t v = threadIdx.x; v < n; v += T)
                 if (!selected(c, v)) sh.dist[v] = mask;
@@ -424,7 +492,9 @@ struct LevelOps {
             const float pct = __fdiv_rn((float)passing, (float)n);
             skip_warmup = pct < (1.0f - kSelectivity);
         }
+        bool bits_ready = false;  // sh.bits holds the vectors below the bound at `cur`
         if (!skip_warmup) {
+            // Warmup (searcher.hpp:374-435); the first step starts the distances from 0
             const uint32_t needed = (uint32_t)ceilf(__fmul_rn(kSelectivity, (float)n));
             uint32_t n_pruned = 0, step = 0;
             while (n_pruned < needed && cur < lv.dv) {
@@ -432,95 +502,167 @@ struct LevelOps {
                 if (last > lv.dv) last = lv.dv;
                 const uint32_t thr = thr_raw(last);
                 count_bytes((unsigned long long)n * (last - cur) * kElem, kWarmup);
-                n_pruned = vertical_all(c, cur, last, true, thr);
+                n_pruned = vertical_all(c, cur, last, true, thr, cur == 0 && !fsel);  // ends with a barrier
                 cur = last;
                 ++step;
+                bits_ready = !fsel;
             }
         }
-        // Prune (searcher.hpp:437-540)
-        uint32_t thr = thr_raw(cur);
+        // Prune (searcher.hpp:437-540): the vectors below the bound at the warmup's last
+        // checkpoint, in position order
+        const uint32_t thr = thr_raw(cur);
         uint32_t* dist = sh.dist;
-        const LevelOps* self = this;  // captured by the predicates
-        uint32_t nsurv = block_compact<T>(
-            n,
-            [&](uint32_t i, uint32_t) { return self->below(dist[i], thr) && self->selected(c, i); },
-            [](uint32_t i) { return i; }, sh.pos, s);
-        uint32_t cur_v = cur, cur_h = 0;
-        while (lv.dh && nsurv && cur_h < lv.dh) {
-            count_bytes((unsigned long long)nsurv * kHDim * kElem, kSurvivorH);
-            horizontal(c, cur_h / kHDim, nsurv, false);
-            cur_h += kHDim;
-            cur += kHDim;
-            thr = thr_raw(cur);
-            uint32_t* pos = sh.pos;
-            nsurv = block_compact<T>(
-                nsurv, [&](uint32_t, uint32_t v) { return self->below(dist[v], thr); },
-                [&](uint32_t i) { return pos[i]; }, sh.pos, s);
+        const LevelOps* self = this;  // captured by the predicate
+        const uint32_t nsurv =
+            bits_ready ? compact_bits(n)
+                       : block_compact<T>(
+                             n,
+                             [&](uint32_t i, uint32_t) { return self->below(dist[i], thr) && self->selected(c, i); },
+                             [](uint32_t i) { return i; }, sh.pos, s);
+        // The bound's heap top is fixed until the merge, so a survivor's way through the
+        // horizontal blocks and the remaining vertical dims depends on that vector alone: each
+        // thread follows whole survivors, and the vectors reaching the merge, and their order,
+        // are those of the reference's block-by-block compaction.
+        uint32_t hbytes = 0, vbytes = 0;
+        for (uint32_t i = threadIdx.x; i < nsurv; i += T) {
+            const uint32_t v = sh.pos[i];
+            uint32_t raw = sh.dist[v];
+            if (follow_survivor(c, v, cur, raw, hbytes, vbytes)) sh.dist[v] = raw;
+            else sh.pos[i] = 0xFFFFFFFFu;
         }
-        while (nsurv && cur_v < lv.dv) {
-            uint32_t last = cur_v + kHDim;
-            if (last > lv.dv) last = lv.dv;
-            count_bytes((unsigned long long)nsurv * (last - cur_v) * kElem, kSurvivorV);
-            vertical_pos(c, cur_v, last, nsurv);
-            cur = (cur + kHDim < lv.d) ? cur + kHDim : lv.d;
-            cur_v = last;
-            thr = thr_raw(cur);
-            uint32_t* pos = sh.pos;
-            nsurv = block_compact<T>(
-                nsurv, [&](uint32_t, uint32_t v) { return self->below(dist[v], thr); },
-                [&](uint32_t i) { return pos[i]; }, sh.pos, s);
-            if (cur == lv.d) break;
+        if (p.stats) {  // block-uniform
+            const uint32_t hb = block_sum<T>(hbytes, s), vb = block_sum<T>(vbytes, s);
+            count_bytes(hb, kSurvivorH);
+            count_bytes(vb, kSurvivorV);
         }
-        if (p.stats && threadIdx.x == 0) s.merged += nsurv;
-        // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, survivor order.
-        if (nsurv) {
+        __syncthreads();
+        // MergeIntoHeap (searcher.hpp:542-566): sequential, strict-<, in position order.
+        if (threadIdx.x < 32 && nsurv) {
+            const uint32_t lane = lane_id();
             const uint32_t* idp = ids(c);
-            if (threadIdx.x < 32) {
-                const uint32_t lane = lane_id();
-                float top = s.top;
-                uint32_t slot = s.top_slot;
-                uint32_t hsize = s.hsize;
-                for (uint32_t i = 0; i < nsurv; ++i) {
-                    const uint32_t v = sh.pos[i];
-                    const float dd = reported(sh.dist[v]);
-                    if (hsize < k || dd < top) {
+            float top = s.top;
+            uint32_t slot = s.top_slot;
+            uint32_t hsize = s.hsize;
+            uint32_t merged = 0;
+            for (uint32_t i0 = 0; i0 < nsurv; i0 += 32) {
+                const uint32_t i = i0 + lane;
+                const uint32_t v = i < nsurv ? sh.pos[i] : 0xFFFFFFFFu;
+                const bool alive = v != 0xFFFFFFFFu;
+                const float dd = alive ? reported(sh.dist[v]) : 0.0f;
+                const uint32_t idv = alive ? __ldg(idp + v) : 0u;
+                unsigned bal = __ballot_sync(0xffffffffu, alive);
+                merged += __popc(bal);
+                while (bal) {
+                    const int j = __ffs(bal) - 1;
+                    bal &= bal - 1;
+                    const float ddj = __shfl_sync(0xffffffffu, dd, j);
+                    const uint32_t idj = __shfl_sync(0xffffffffu, idv, j);
+                    if (hsize < k || ddj < top) {
                         if (lane == 0) {
                             const uint32_t at = (hsize >= k) ? slot : hsize;
-                            sh.hd[at] = dd;
-                            sh.hid[at] = __ldg(idp + v);
+                            sh.hd[at] = ddj;
+                            sh.hid[at] = idj;
                         }
                         if (hsize < k) ++hsize;
                         __syncwarp();
-                        float best = -1.0f;
-                        uint32_t bs = 0xFFFFFFFFu;
-                        for (uint32_t j = lane; j < hsize; j += 32) {
-                            const float x = sh.hd[j];
-                            if (x > best || (x == best && j < bs)) {
-                                best = x;
-                                bs = j;
-                            }
-                        }
-#pragma unroll
-                        for (int off = 16; off > 0; off >>= 1) {
-                            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-                            const uint32_t os = __shfl_xor_sync(0xffffffffu, bs, off);
-                            if (ob > best || (ob == best && os < bs)) {
-                                best = ob;
-                                bs = os;
-                            }
-                        }
-                        top = best;
-                        slot = bs;
+                        warp_heap_top(hsize, top, slot);
                     }
                 }
-                if (lane == 0) {
-                    s.top = top;
-                    s.top_slot = slot;
-                    s.hsize = hsize;
-                }
             }
-            __syncthreads();
+            if (lane == 0) {
+                s.top = top;
+                s.top_slot = slot;
+                s.hsize = hsize;
+                if (p.stats) s.merged += merged;
+            }
         }
+        __syncthreads();
+    }
+
+    // Raw distance of vector v plus horizontal block b (searcher.hpp:437-540 per vector).
+    __device__ __forceinline__ uint32_t add_hblock(const DevCluster& c, uint32_t b, uint32_t v, uint32_t raw) const {
+        const uint32_t np = c.n_pad;
+        if constexpr (U8) {
+            const uint4* row = reinterpret_cast<const uint4*>(p.arena + c.hor_off + ((size_t)b * np + v) * kHDim);
+            const uint4* qh = reinterpret_cast<const uint4*>(sh.qw + lv.qw_hoff + b * 16);
+            uint4 x[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) x[t] = __ldg(row + t);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const uint4 q4 = qh[t];
+                raw = sqdiff4(q4.x, x[t].x, raw);
+                raw = sqdiff4(q4.y, x[t].y, raw);
+                raw = sqdiff4(q4.z, x[t].z, raw);
+                raw = sqdiff4(q4.w, x[t].w, raw);
+            }
+            return raw;
+        } else {
+            // avx2_computers.hpp:47-98: lane j of 8 accumulates dims j, j + 8, ... with FMA;
+            // lanes j and j + 4 are added in double, then (0 + 2) + (1 + 3)
+            const float* row = reinterpret_cast<const float*>(p.arena + c.hor_off) + ((size_t)b * np + v) * kHDim;
+            const float* qh = sh.qf + lv.dv + b * kHDim;
+            double sj[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const float d0 = __fsub_rn(qh[j + 8 * t], __ldg(row + j + 8 * t));
+                    a0 = __fmaf_rn(d0, d0, a0);
+                    const float d1 = __fsub_rn(qh[j + 4 + 8 * t], __ldg(row + j + 4 + 8 * t));
+                    a1 = __fmaf_rn(d1, d1, a1);
+                }
+                sj[j] = (double)a0 + (double)a1;
+            }
+            const float h = (float)((sj[0] + sj[2]) + (sj[1] + sj[3]));
+            return __float_as_uint(__fadd_rn(__uint_as_float(raw), h));
+        }
+    }
+
+    // Raw distance of vector v plus vertical dims [d0, d1) in dimension order.
+    __device__ __forceinline__ uint32_t add_vertical(const DevCluster& c, uint32_t v, uint32_t d0, uint32_t d1,
+                                                     uint32_t raw) const {
+        const uint32_t* base = vert(c);
+        const uint32_t np = c.n_pad;
+        if constexpr (U8) {
+            const uint32_t g0 = d0 >> 2, g1 = (d1 + 3) >> 2;
+            for (uint32_t g = g0; g < g1; ++g) raw = sqdiff4(sh.qw[g], __ldg(base + (size_t)g * np + v), raw);
+            return raw;
+        } else {
+            const float* fb = reinterpret_cast<const float*>(base);
+            float acc = __uint_as_float(raw);
+            for (uint32_t j = d0; j < d1; ++j) {
+                const float t = __fsub_rn(sh.qf[j], __ldg(fb + (size_t)j * np + v));
+                acc = __fmaf_rn(t, t, acc);
+            }
+            return __float_as_uint(acc);
+        }
+    }
+
+    // One survivor of the warmup bound from checkpoint cur0 on: the horizontal blocks, then the
+    // remaining vertical dims in 64-dim steps, re-tested after each (searcher.hpp:437-540).
+    // Returns whether it is still below the bound at the end; raw is its running distance.
+    __device__ __forceinline__ bool follow_survivor(const DevCluster& c, uint32_t v, uint32_t cur0, uint32_t& raw,
+                                                    uint32_t& hbytes, uint32_t& vbytes) const {
+        uint32_t cur = cur0;
+        for (uint32_t b = 0; b < lv.n_hblocks; ++b) {
+            hbytes += kHDim * kElem;
+            raw = add_hblock(c, b, v, raw);
+            cur += kHDim;
+            if (!below(raw, thr_raw(cur))) return false;
+        }
+        uint32_t cur_v = cur0;
+        while (cur_v < lv.dv) {
+            const uint32_t last = (cur_v + kHDim < lv.dv) ? cur_v + kHDim : lv.dv;
+            vbytes += (last - cur_v) * kElem;
+            raw = add_vertical(c, v, cur_v, last, raw);
+            cur = (cur + kHDim < lv.d) ? cur + kHDim : lv.d;
+            cur_v = last;
+            if (!below(raw, thr_raw(cur))) return false;
+            if (cur == lv.d) break;
+        }
+        return true;
     }
 
     // Visits clusters order[0, nvisit) (searcher.hpp:655-721 / 776-853).
@@ -546,6 +688,8 @@ struct LevelOps {
                 if (p.stats && threadIdx.x == 0) t0 = clock64();
                 if (fsel)
                     filtered_start(c, k, passing);
+                else if (pre_row >= 0 && s.hsize == 0 && cidx == pre_cluster)
+                    start_pre(c, k);
                 else
                     start(c, k);
                 if (p.stats && threadIdx.x == 0 && !top_level)
@@ -619,29 +763,7 @@ __device__ void prepare_query(const SearchParams& p, Shared& sh, uint32_t q) {
     if (lv.is_u8) {
         // QuantizeEmbedding (scalar.hpp:76-94), packed into the device word layout
         const uint32_t nw = lv.qw_hoff + lv.n_hblocks * 16;
-        for (uint32_t w = threadIdx.x; w < nw; w += T) {
-            uint32_t word = 0;
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                uint32_t dim;
-                bool valid;
-                if (w < lv.qw_hoff) {
-                    dim = w * 4 + b;
-                    valid = dim < lv.dv;
-                } else {
-                    dim = lv.dv + (w - lv.qw_hoff) * 4 + b;
-                    valid = true;
-                }
-                uint32_t byte = 0;
-                if (valid) {
-                    const float v = __fmul_rn(__fsub_rn(sh.qf[dim], lv.base), lv.scale);
-                    const int r = (int)roundf(v);
-                    byte = r > 255 ? 255u : (r < 0 ? 0u : (uint32_t)r);
-                }
-                word |= byte << (8 * b);
-            }
-            sh.qw[w] = word;
-        }
+        for (uint32_t w = threadIdx.x; w < nw; w += T) sh.qw[w] = quantize_word(sh.qf, lv, w);
         __syncthreads();
     }
 }
@@ -660,6 +782,7 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
     sh.hid = reinterpret_cast<uint32_t*>(smem + p.smem_heap) + p.heap_cap;
     sh.sorth = reinterpret_cast<uint64_t*>(smem + p.smem_heap);
     sh.order = reinterpret_cast<uint32_t*>(smem + p.smem_order);
+    sh.bits = reinterpret_cast<uint32_t*>(smem + p.smem_bits);
 
     for (;;) {
         if (threadIdx.x == 0) s.query = atomicAdd(p.queue, 1u);
@@ -716,6 +839,10 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             t_q0 = now;
         }
         LevelOps<T, U8> ops(p, p.l1, sh, s, filter);
+        if (U8 && p.start_row && filter == -1) {
+            ops.pre_row = __ldg(p.start_row + q);
+            ops.pre_cluster = __ldg(p.start_first + q);
+        }
         ops.run(kq, nvisit);
         const uint32_t cnt = ops.sort_heap(kq);
         uint32_t* oi = p.out_ids + (size_t)q * p.k;
@@ -769,6 +896,7 @@ __global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ Se
     sh.hid = reinterpret_cast<uint32_t*>(smem + p.smem_heap) + p.heap_cap;
     sh.sorth = reinterpret_cast<uint64_t*>(smem + p.smem_heap);
     sh.order = reinterpret_cast<uint32_t*>(smem + p.smem_order);
+    sh.bits = reinterpret_cast<uint32_t*>(smem + p.smem_bits);
     uint32_t* out_order = const_cast<uint32_t*>(p.q_order);
     uint32_t* out_count = const_cast<uint32_t*>(p.q_order_count);
     for (;;) {
@@ -851,6 +979,7 @@ static int occupancy_t(bool u8, size_t smem) {
 
 int search_occupancy(bool u8, int threads, size_t smem) {
     switch (threads) {
+    case 64: return occupancy_t<64>(u8, smem);
     case 128: return occupancy_t<128>(u8, smem);
     case 256: return occupancy_t<256>(u8, smem);
     case 512: return occupancy_t<512>(u8, smem);
@@ -860,6 +989,7 @@ int search_occupancy(bool u8, int threads, size_t smem) {
 
 cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid, cudaStream_t st) {
     switch (threads) {
+    case 64: return u8 ? launch_t<true, 64>(p, grid, st) : launch_t<false, 64>(p, grid, st);
     case 128: return u8 ? launch_t<true, 128>(p, grid, st) : launch_t<false, 128>(p, grid, st);
     case 256: return u8 ? launch_t<true, 256>(p, grid, st) : launch_t<false, 256>(p, grid, st);
     case 512: return u8 ? launch_t<true, 512>(p, grid, st) : launch_t<false, 512>(p, grid, st);

@@ -115,7 +115,7 @@ def test_fresh_vs_port_dims(port_cls, itype, d):
 def test_fresh_vs_port_k_and_threads(port_cls, itype):
     f, X, Q = _fresh(itype, 160, 3000, 20, 4, norm=True, seed=4)
     for k in (1, 7, 100):
-        _compare_with_port(port_cls, f, Q, k, (0, 1, 6, 25), threads=(128, 256, 512))
+        _compare_with_port(port_cls, f, Q, k, (0, 1, 6, 25), threads=(64, 128, 256, 512))
 
 
 @pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8", "pdx_tree_u8"])
@@ -313,6 +313,51 @@ def test_tree_top_level_tiled_stats_match():
         assert out[2][0]["clusters_visited"] == out[3][0]["clusters_visited"]
         np.testing.assert_array_equal(out[2][1], out[3][1])
         np.testing.assert_array_equal(out[2][2], out[3][2])
+
+
+@pytest.mark.parametrize("top_mode", [2, 3])
+def test_batched_start_matches_scan_start(port_cls, top_mode):
+    """The batched first-cluster Start (exact U8 distances computed once per cluster and query
+    group) gives the same results, and the same algorithmic byte count, as the scan's own
+    Start, and the oracle's results; k above the first cluster's size continues with the
+    scan's Start on the next clusters."""
+    import torch
+    gm = GaussianMixture(256, 30, 0.4, seed=13, unit_norm=True)
+    X = gm.sample(8000, 0)
+    Q = gm.sample(200, 1)
+    f = build_index(X, "pdx_tree_u8", num_clusters=64, num_meso_clusters=8, normalize=True, seed=6)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        port = port_cls(p)
+        ix = compiled.load_index(p)
+        ix.set_top_level_mode(top_mode)
+        R = ix.prepare_queries(Q)
+        Rd = torch.from_numpy(R).cuda()
+        nq = len(Q)
+        for nprobe, k in ((6, 10), (20, 500)):
+            ix.set_nprobe(nprobe)
+            port.set_nprobe(nprobe)
+            ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+            ds = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+            cnt = torch.empty(nq, dtype=torch.int32, device="cuda")
+            out = {}
+            for mode in (1, 0):
+                ix.set_start_mode(mode)
+                ix.search_device(Rd.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(),
+                                 stream=torch.cuda.current_stream().cuda_stream, transformed=True, stats=True)
+                torch.cuda.synchronize()
+                out[mode] = (ix.last_stats(), ix.last_launch_count(), ids.cpu().numpy().copy(),
+                             ds.cpu().numpy().copy(), cnt.cpu().numpy().copy())
+            assert out[0][1] == out[1][1] + 3  # count, plan and distance kernels ran
+            assert out[0][0]["bytes_by_phase"] == out[1][0]["bytes_by_phase"]
+            for j in (2, 3, 4):
+                np.testing.assert_array_equal(out[0][j], out[1][j])
+            gi, gd, gc = out[0][2].view(np.uint32), out[0][3], out[0][4]
+            for i in range(0, nq, 7):
+                pi, pd = port.search(R[i], k, transformed=True)
+                assert_same(gi[i, :gc[i]], gd[i, :gc[i]], pi, pd, ctx=f"top_mode={top_mode} k={k} q{i}")
+        port.close()
 
 
 def test_tree_top_level_batched_edge_sizes(port_cls):
