@@ -191,6 +191,22 @@ int pdxg_set_top_level_mode(pdxg_index* index, uint32_t mode);
  * scan CTA. Results are identical in both modes. No counterpart in the reference. */
 int pdxg_set_start_mode(pdxg_index* index, uint32_t mode);
 
+/* The centroid probe (GetClustersAccessOrderIVF, searcher.hpp:181-215; for tree indexes the
+ * top-level search of PDXTreeIndex::Search, index.hpp:545-566). 0 = the reference's (default);
+ * 1 = reduced precision: the rotation and the scores against every L1 centroid run as BF16
+ * tensor-core GEMMs with FP32 accumulation, the nprobe list is widened by 10 %, and those
+ * candidates are rescored in FP32 with the reference's arithmetic to keep the nprobe nearest;
+ * 2 = the same with FP8-E4M3 centroid scores. Modes 1 and 2 need tensor cores and d a multiple
+ * of 16 (PDXG_ERR_UNSUPPORTED otherwise); their results differ from the reference's where the
+ * reduced precision changes a probe set or a quantized query. No counterpart in the reference
+ * (a precision form of its probe). */
+int pdxg_set_probe_mode(pdxg_index* index, uint32_t mode);
+
+/* The L1 visit orders of the last pdxg_search_device call, when it computed them ahead of the
+ * scan (tree top level in its own launch, or probe modes 1 and 2): orders[i * stride + j] for
+ * j < counts[i]. Waits for the device. No counterpart in the reference. */
+int pdxg_last_visit_orders(pdxg_index* index, uint32_t nq, uint32_t stride, uint32_t* orders, uint32_t* counts);
+
 /* ---------------------------------------------------------------------------------------
  * Serving-style batches. A context owns a workspace and a CUDA stream; work issued on
  * different contexts of one index runs concurrently. No counterpart in the reference (one

@@ -56,6 +56,8 @@ def library() -> C.CDLL:
         fn("pdxg_set_top_level_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_last_launch_count", C.c_uint32, vp)
         fn("pdxg_set_start_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_set_probe_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_last_visit_orders", C.c_int, vp, C.c_uint32, C.c_uint32, vp, vp)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
         fn("pdxg_search_with_order", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, _u32p, C.c_uint32,
@@ -329,6 +331,19 @@ class PDXIndex:
     def set_start_mode(self, mode: int) -> None:
         """U8 tree indexes: 0 batched first-cluster Start when it fits, 1 inside the scan."""
         _check(library().pdxg_set_start_mode(self._handle().ptr, int(mode)))
+
+    def set_probe_mode(self, mode: int) -> None:
+        """0 reference probe; 1 BF16 tensor-core rotation + centroid scores, widened list, FP32
+        rescore; 2 the same with FP8-E4M3 centroid scores."""
+        _check(library().pdxg_set_probe_mode(self._handle().ptr, int(mode)))
+
+    def last_visit_orders(self, nq: int, nprobe: int):
+        """Visit orders computed ahead of the scan by the last search_device call."""
+        orders = np.zeros((nq, nprobe), np.uint32)
+        counts = np.zeros(nq, np.uint32)
+        _check(library().pdxg_last_visit_orders(self._handle().ptr, nq, nprobe, orders.ctypes.data,
+                                                counts.ctypes.data))
+        return orders, counts
 
     def set_rotation_mode(self, mode: int) -> None:
         """0: tcgen05 TF32x3 rotation when available, 1: FP32 SIMT GEMM."""

@@ -131,6 +131,23 @@ struct TopLevelParams {
     uint32_t probe_q;            // queries per meso probe CTA (1..8)
 };
 
+// Reduced-precision centroid probe (pdxg_probe.cu).
+struct ProbeParams {
+    const float* queries;        // prepared queries [nq x d] (FP32)
+    const float* centroids;      // [nclusters x d] FP32
+    const float* scores;         // [nq x ld_scores] approximate |c|^2 - 2 q.c
+    uint32_t ld_scores;
+    uint32_t nq, d, nclusters;
+    uint32_t nprobe;             // resolved nprobe (row stride of order)
+    const uint32_t* q_nprobe;    // optional per-query resolved nprobe (<= nprobe)
+    uint32_t* order;             // [nq x stride] clusters to visit, nearest first
+    uint32_t stride;
+    uint32_t* count;             // [nq]
+    uint32_t cand_cap, sort_cap; // shared-memory capacities (candidates, sort keys)
+    uint32_t score_bytes;        // bytes per centroid element read by the approximate scores
+    unsigned long long* stats;   // optional, SearchParams::stats layout
+};
+
 // Batched Start (pdxg_start.cu).
 struct StartParams {
     const uint8_t* arena;

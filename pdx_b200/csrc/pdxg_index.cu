@@ -30,6 +30,9 @@ int top_level_occupancy(size_t smem);
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
                                    cudaStream_t st);
 cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t st);
+cudaError_t launch_row_sq(const float* x, uint32_t n, uint32_t d, float* out, cudaStream_t st);
+size_t probe_select_smem(uint32_t d, uint32_t n1, uint32_t cand_cap, uint32_t sort_cap);
+cudaError_t launch_probe_select(const ProbeParams& pp, cudaStream_t st);
 int start_dist_occupancy(size_t smem);
 size_t start_dist_smem(const DevLevel& lv);
 uint64_t start_item_bound(uint32_t nq, uint32_t n1, uint32_t max_n);
@@ -283,6 +286,17 @@ struct Workspace {
     uint64_t st_items_cap = 0;
     uint32_t* d_st_dist = nullptr;
     uint64_t st_dist_cap = 0;
+    // reduced-precision probe: BF16 queries, BF16 / E4M3 rotated queries (+ row scales), scores
+    uint16_t* d_pq_b16 = nullptr;
+    uint64_t pq_b16_cap = 0;
+    uint16_t* d_pq_r16 = nullptr;
+    uint64_t pq_r16_cap = 0;
+    uint8_t* d_pq_r8 = nullptr;
+    uint64_t pq_r8_cap = 0;
+    float* d_pq_r8s = nullptr;
+    uint64_t pq_r8s_cap = 0;
+    float* d_pq_scores = nullptr;
+    uint64_t pq_scores_cap = 0;
     // per-query request parameters (pdxg_search_requests)
     uint32_t* d_req = nullptr;  // q_k | q_nprobe | q_top | filter_of, nq each
     uint64_t req_cap = 0;
@@ -301,7 +315,8 @@ void free_workspace(Workspace& w) {
     void* ptrs[] = {w.d_q, w.d_rq, w.d_norms, w.d_ids, w.d_dists, w.d_counts, w.d_queue, w.d_order,
                     w.d_sel, w.d_pass, w.d_filter_of, w.d_stats, w.d_top_order, w.d_top_off,
                     w.d_top_lists, w.d_top_count, w.d_top_vals, w.d_l1_order, w.d_l1_count,
-                    w.d_st_cl, w.d_st_q, w.d_st_items, w.d_st_dist,
+                    w.d_st_cl, w.d_st_q, w.d_st_items, w.d_st_dist, w.d_pq_b16, w.d_pq_r16, w.d_pq_r8,
+                    w.d_pq_r8s, w.d_pq_scores,
                     w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
     for (void* q : ptrs) cudaFree(q);
     w = Workspace();
@@ -339,6 +354,17 @@ struct pdxg_index {
     uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch of
                             // per-query CTAs, 3 tiled (probe, partials, replay)
     uint32_t start_mode = 0;  // U8 first-cluster Start: 0 batched when it fits, 1 in the scan
+    // centroid probe: 0 the reference's (exact FP32 probe / tree top-level search), 1 BF16
+    // tensor-core rotation and centroid scores + widened list + FP32 rescore, 2 the same with
+    // FP8-E4M3 centroid scores. Operands are built on first use.
+    uint32_t probe_mode = 0;
+    bool pp_ready = false;
+    void* d_rot_b16 = nullptr;   // M^T, BF16 (K-major B operand of the rotation)
+    void* d_c1_b16 = nullptr;    // L1 centroids, BF16
+    uint8_t* d_c1_e4 = nullptr;  // L1 centroids, E4M3 with one scale per row
+    float* d_c1_e4s = nullptr;
+    float* d_c1_sq = nullptr;    // |c|^2 of the FP32 L1 centroids
+    GemmOperand rot_op16{}, c1_op16{}, c1_op8{};
     int num_sms = 0;
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
@@ -347,6 +373,7 @@ struct pdxg_index {
     cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // PDXG_TIME_KERNELS marks
     bool tev_ready = false, tev_top = false, tev_prep = false;
     uint32_t last_launches = 0;  // engine kernels launched by the last search_device_impl
+    uint32_t last_order_stride = 0;  // row stride of the visit orders of the last search (0: none)
     Workspace ws;
     std::mutex mu;
     // registered filters (pdxg_filter_register): resident selection bitmaps + passing counts,
@@ -411,6 +438,11 @@ void free_index(pdxg_index* ix) {
     cudaFree(ix->d_cent0);
     cudaFree(ix->d_rot);
     cudaFree(ix->d_rot_hi);
+    cudaFree(ix->d_rot_b16);
+    cudaFree(ix->d_c1_b16);
+    cudaFree(ix->d_c1_e4);
+    cudaFree(ix->d_c1_e4s);
+    cudaFree(ix->d_c1_sq);
     cudaFree(ix->d_rot_lo);
     cudaFree(ix->d_ratios);
     cudaFree(ix->d_rid_cluster);
@@ -636,6 +668,7 @@ struct Launch {
     int grid = 1;
     uint32_t top_launches = 0;  // kernels of a separate tree top level
     uint32_t start_launches = 0;  // kernels of the batched Start
+    uint32_t probe_launches = 0;  // kernels of the reduced-precision probe (rotation included)
 };
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
@@ -933,6 +966,136 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     return PDXG_OK;
 }
 
+uint16_t bf16_rne(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
+}
+
+// Whether the reduced-precision probe can run on this index (tensor cores, d a multiple of
+// 16, candidate arrays within shared memory).
+bool probe_gemm_ok(const pdxg_index* ix) {
+    const uint32_t n1 = (uint32_t)ix->l1.fc.size();
+    return gemm_available() && ix->d % 16 == 0 && gemm_shape_ok(kGemmBF16, ix->d) && gemm_shape_ok(kGemmE4M3, ix->d) &&
+           probe_select_smem(ix->d, n1, (n1 + 3) & ~3u, next_pow2(n1)) + 2048 <= ix->max_smem;
+}
+
+int prepare_probe_gemm(pdxg_index* ix, cudaStream_t st) {
+    if (ix->pp_ready) return PDXG_OK;
+    const uint32_t d = ix->d, n1 = (uint32_t)ix->l1.fc.size();
+    std::vector<uint16_t> rt((size_t)d * d);
+    for (uint32_t i = 0; i < d; ++i)
+        for (uint32_t j = 0; j < d; ++j) rt[(size_t)j * d + i] = bf16_rne(ix->rotation[(size_t)i * d + j]);
+    PDXG_CUDA(cudaMalloc(&ix->d_rot_b16, rt.size() * 2));
+    PDXG_CUDA(cudaMemcpy(ix->d_rot_b16, rt.data(), rt.size() * 2, cudaMemcpyHostToDevice));
+    PDXG_CUDA(cudaMalloc(&ix->d_c1_b16, (size_t)n1 * d * 2));
+    PDXG_CUDA(cudaMalloc(&ix->d_c1_e4, (size_t)n1 * d));
+    PDXG_CUDA(cudaMalloc(&ix->d_c1_e4s, (size_t)n1 * 4));
+    PDXG_CUDA(cudaMalloc(&ix->d_c1_sq, (size_t)n1 * 4));
+    PDXG_CUDA(launch_bf16_rows(ix->d_cent1, n1, d, false, ix->d_c1_b16, st));
+    PDXG_CUDA(launch_e4m3_rows(ix->d_cent1, n1, d, ix->d_c1_e4, ix->d_c1_e4s, st));
+    PDXG_CUDA(launch_row_sq(ix->d_cent1, n1, d, ix->d_c1_sq, st));
+    if (make_gemm_operand(ix->rot_op16, kGemmBF16, ix->d_rot_b16, nullptr, d, d) != 0 ||
+        make_gemm_operand(ix->c1_op16, kGemmBF16, ix->d_c1_b16, nullptr, n1, d) != 0 ||
+        make_gemm_operand(ix->c1_op8, kGemmE4M3, ix->d_c1_e4, nullptr, n1, d) != 0)
+        return fail(PDXG_ERR_CUDA, "cannot encode the probe tensor maps");
+    ix->pp_ready = true;
+    return PDXG_OK;
+}
+
+// Reduced-precision probe (probe modes 1 and 2): BF16 rotation of the raw queries into w.d_rq
+// (skipped for transformed queries), tensor-core centroid scores, widened list, FP32 rescore.
+// Sets L.p.queries to the rotated queries and L.p.q_order to the visit orders.
+int run_probe_gemm(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, bool transformed, Launch& L,
+                   cudaStream_t st) {
+    const uint32_t d = ix->d, n1 = L.p.l1.nclusters;
+    int rc;
+    if ((rc = prepare_probe_gemm(ix, st))) return rc;
+    if (!w.d_gemm_err) {
+        PDXG_CUDA(cudaMalloc(&w.d_gemm_err, sizeof(int)));
+        PDXG_CUDA(cudaMemsetAsync(w.d_gemm_err, 0, sizeof(int), st));
+    }
+    if ((rc = dev_grow(w.d_pq_r16, w.pq_r16_cap, (uint64_t)nq * d))) return rc;
+    if ((rc = dev_grow(w.d_pq_scores, w.pq_scores_cap, (uint64_t)nq * n1))) return rc;
+    const float* rq = q;
+    if (!transformed) {
+        // NormalizeQuery + Rotate as one BF16 GEMM, FP32 accumulation; BF16 copy for the scores
+        if ((rc = dev_grow(w.d_pq_b16, w.pq_b16_cap, (uint64_t)nq * d))) return rc;
+        PDXG_CUDA(launch_bf16_rows(q, nq, d, ix->normalized, w.d_pq_b16, st));
+        GemmOperand a;
+        if (make_gemm_operand(a, kGemmBF16, w.d_pq_b16, nullptr, nq, d) != 0)
+            return fail(PDXG_ERR_CUDA, "cannot encode the query tensor map");
+        GemmArgs g{};
+        g.M = nq;
+        g.N = d;
+        g.K = d;
+        g.out = w.d_rq;
+        g.ldo = d;
+        g.out_b16 = w.d_pq_r16;
+        g.ldo16 = d;
+        g.error = w.d_gemm_err;
+        PDXG_CUDA(launch_gemm(a, ix->rot_op16, kEpiStore, g, st));
+        rq = w.d_rq;
+        L.probe_launches += 2;
+    } else {
+        PDXG_CUDA(launch_bf16_rows(q, nq, d, false, w.d_pq_r16, st));
+        L.probe_launches += 1;
+    }
+    GemmArgs g{};
+    g.M = nq;
+    g.N = n1;
+    g.K = d;
+    g.out = w.d_pq_scores;
+    g.ldo = n1;
+    g.col_add = ix->d_c1_sq;
+    g.error = w.d_gemm_err;
+    if (ix->probe_mode == 2) {
+        if ((rc = dev_grow(w.d_pq_r8, w.pq_r8_cap, (uint64_t)nq * d))) return rc;
+        if ((rc = dev_grow(w.d_pq_r8s, w.pq_r8s_cap, nq))) return rc;
+        PDXG_CUDA(launch_e4m3_rows(rq, nq, d, w.d_pq_r8, w.d_pq_r8s, st));
+        GemmOperand a;
+        if (make_gemm_operand(a, kGemmE4M3, w.d_pq_r8, nullptr, nq, d) != 0)
+            return fail(PDXG_ERR_CUDA, "cannot encode the query tensor map");
+        g.row_scale = w.d_pq_r8s;
+        g.col_scale = ix->d_c1_e4s;
+        PDXG_CUDA(launch_gemm(a, ix->c1_op8, kEpiDist, g, st));
+        L.probe_launches += 2;
+    } else {
+        GemmOperand a;
+        if (make_gemm_operand(a, kGemmBF16, w.d_pq_r16, nullptr, nq, d) != 0)
+            return fail(PDXG_ERR_CUDA, "cannot encode the query tensor map");
+        PDXG_CUDA(launch_gemm(a, ix->c1_op16, kEpiDist, g, st));
+        L.probe_launches += 1;
+    }
+    const uint32_t k1 = L.p.nprobe;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    ProbeParams pp{};
+    pp.queries = rq;
+    pp.centroids = ix->d_cent1;
+    pp.scores = w.d_pq_scores;
+    pp.ld_scores = n1;
+    pp.nq = nq;
+    pp.d = d;
+    pp.nclusters = n1;
+    pp.nprobe = k1;
+    pp.q_nprobe = L.p.q_nprobe;
+    pp.order = w.d_l1_order;
+    pp.stride = k1;
+    pp.count = w.d_l1_count;
+    pp.cand_cap = (n1 + 3) & ~3u;
+    pp.sort_cap = next_pow2(n1);
+    pp.score_bytes = ix->probe_mode == 2 ? 1u : 2u;
+    pp.stats = L.p.stats;
+    PDXG_CUDA(launch_probe_select(pp, st));
+    L.probe_launches += 1;
+    L.p.queries = rq;
+    L.p.q_order = w.d_l1_order;
+    L.p.q_order_count = w.d_l1_count;
+    L.p.q_order_stride = k1;
+    return PDXG_OK;
+}
+
 // Batched Start (pdxg_start.cu) for U8 levels whose visit orders are known before the scan
 // (tree indexes with a separate top level). Sets L.p.start_* when it ran; a batch outside its
 // limits leaves them unset and the scan runs Start itself.
@@ -1004,9 +1167,11 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         PDXG_CUDA(cudaEventRecord(ix->tev[0], st));
     }
     const float* qp = q;
-    ix->tev_prep = !(flags & PDXG_QUERY_TRANSFORMED);
+    // the reduced-precision probe rotates the queries itself (BF16 GEMM)
+    const bool gemm_probe = ix->probe_mode != 0 && !d_order && probe_gemm_ok(ix);
+    ix->tev_prep = !(flags & PDXG_QUERY_TRANSFORMED) && !gemm_probe;
     uint32_t launches = 1;  // the scan
-    if (!(flags & PDXG_QUERY_TRANSFORMED)) {
+    if (!(flags & PDXG_QUERY_TRANSFORMED) && !gemm_probe) {
         if ((rc = prepare_dev(ix, w, q, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
         // TF32 split + tensor-core GEMM, or [norms +] SIMT GEMM
@@ -1032,12 +1197,18 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         L.p.stats = w.d_stats;
         ix->stats_stream = st;
     }
-    if (ix->tree && !any_filter && !d_order) {
+    if (gemm_probe) {
+        rc = run_probe_gemm(ix, w, q, nq, (flags & PDXG_QUERY_TRANSFORMED) != 0, L, st);
+        if (rc) return rc;
+        qp = L.p.queries;
+        launches += L.probe_launches;
+    } else if (ix->tree && !any_filter && !d_order) {
         rc = run_top_level(ix, w, qp, nq, L, st);
         if (rc) return rc;
         launches += L.top_launches;
     }
     ix->tev_top = L.p.q_order != nullptr;
+    ix->last_order_stride = L.p.q_order ? L.p.q_order_stride : 0;
     // the batched Start belongs to the scan's time
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
     if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
@@ -1213,6 +1384,32 @@ int pdxg_set_top_level_mode(pdxg_index* ix, uint32_t mode) {
     if (int rc = check_index(ix)) return rc;
     if (mode > 3) return fail(PDXG_ERR_INVALID_ARGUMENT, "top-level mode must be 0, 1, 2 or 3");
     ix->top_mode = mode;
+    return PDXG_OK;
+}
+
+int pdxg_set_probe_mode(pdxg_index* ix, uint32_t mode) {
+    if (int rc = check_index(ix)) return rc;
+    if (mode > 2) return fail(PDXG_ERR_INVALID_ARGUMENT, "probe mode must be 0, 1 or 2");
+    if (mode != 0 && !probe_gemm_ok(ix))
+        return fail(PDXG_ERR_UNSUPPORTED, "the reduced-precision probe needs tensor cores and d a multiple of 16");
+    ix->probe_mode = mode;
+    return PDXG_OK;
+}
+
+int pdxg_last_visit_orders(pdxg_index* ix, uint32_t nq, uint32_t stride, uint32_t* orders, uint32_t* counts) {
+    if (int rc = check_index(ix)) return rc;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (!ix->ws.d_l1_order || !ix->ws.d_l1_count || (uint64_t)nq * ix->last_order_stride > ix->ws.l1_order_cap ||
+        nq > ix->ws.l1_count_cap || ix->last_order_stride == 0)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "no visit orders of that size were computed by the last search");
+    if (stride < ix->last_order_stride) return fail(PDXG_ERR_INVALID_ARGUMENT, "stride below the last nprobe");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    PDXG_CUDA(cudaDeviceSynchronize());
+    std::vector<uint32_t> h((size_t)nq * ix->last_order_stride);
+    PDXG_CUDA(cudaMemcpy(h.data(), ix->ws.d_l1_order, h.size() * 4, cudaMemcpyDeviceToHost));
+    PDXG_CUDA(cudaMemcpy(counts, ix->ws.d_l1_count, (size_t)nq * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nq; ++i)
+        std::memcpy(orders + (size_t)i * stride, h.data() + (size_t)i * ix->last_order_stride, ix->last_order_stride * 4);
     return PDXG_OK;
 }
 
@@ -1659,7 +1856,8 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
         PDXG_CUDA(cudaGetLastError());
     }
     const float* qp = queries;
-    if (!(flags & PDXG_QUERY_TRANSFORMED)) {
+    const bool gemm_probe = ix->probe_mode != 0 && probe_gemm_ok(ix);
+    if (!(flags & PDXG_QUERY_TRANSFORMED) && !gemm_probe) {
         if ((rc = prepare_dev(ix, w, queries, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
     }
@@ -1680,7 +1878,11 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
     L.p.out_dists = distances;
     L.p.out_counts = counts;
     L.p.queue = w.d_queue;
-    if (ix->tree && any_plain) {
+    if (gemm_probe) {
+        if ((rc = run_probe_gemm(ix, w, queries, nq, (flags & PDXG_QUERY_TRANSFORMED) != 0, L, st))) return rc;
+        qp = L.p.queries;
+        if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
+    } else if (ix->tree && any_plain) {
         if ((rc = run_top_level(ix, w, qp, nq, L, st))) return rc;
         if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
     }

@@ -811,8 +811,9 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             nvisit = npq < p.n_order ? npq : p.n_order;
             for (uint32_t i = threadIdx.x; i < nvisit; i += T) sh.order[i] = __ldg(p.order + i);
             __syncthreads();
-        } else if (p.is_tree && filter == -1 && p.q_order) {
-            // batched tree top level (pdxg_toplevel.cu) already produced this query's L1 order
+        } else if (filter == -1 && p.q_order) {
+            // the tree top level (pdxg_toplevel.cu) or the reduced-precision probe
+            // (pdxg_probe.cu) already produced this query's L1 order
             nvisit = __ldg(p.q_order_count + q);
             for (uint32_t i = threadIdx.x; i < nvisit; i += T)
                 sh.order[i] = __ldg(p.q_order + (size_t)q * p.q_order_stride + i);
