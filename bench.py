@@ -50,6 +50,12 @@ CONFIGS = {
     "flat_f32_2m_d768": dict(itype="pdx_f32", n=2_000_000, d=768, comps=2048, sigma=0.2, seed=3,
                              unit=True, normalize=True, nlist=5657, nmeso=0, nprobe=0, k=100,
                              nq=1024),
+    # precision form of the IVF2 SQ8 workload: BF16 tensor-core rotation and L1 centroid scores,
+    # probe list widened by 10 %, FP32 rescore; 1,024-query batches over the same index
+    "precision_ivf2_sq8_1m_d1024": dict(itype="pdx_tree_u8", n=1_000_000, d=1024, comps=1024,
+                                        sigma=0.25, seed=2, unit=True, normalize=True, nlist=1000,
+                                        nmeso=32, nprobe=32, k=20, nq=1024, probe_mode=1,
+                                        dataset="ivf2_sq8_1m_d1024"),
 }
 DEFAULT_CONFIG = "ivf2_sq8_1m_d1024"
 CACHE = os.environ.get("PDXG_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "pdxg_bench"))
@@ -65,6 +71,7 @@ def dataset(name: str, device: str):
     """Index file, query generator and ground truth, built once and cached on local disk."""
     from pdx_b200.builder import GaussianMixture, build_index
     cfg = CONFIGS[name]
+    name = cfg.get("dataset", name)  # workloads over the same index share its files
     os.makedirs(CACHE, exist_ok=True)
     path = os.path.join(CACHE, f"{name}.pdx")
     gt_path = os.path.join(CACHE, f"{name}.gt.npy")
@@ -200,6 +207,8 @@ def main():
                     help="tree top level: 0 auto, 1 per query, 2 batched warp-per-query kernel")
     ap.add_argument("--rotation-mode", type=int, default=None,
                     help="0: tcgen05 TF32x3 rotation when available (default), 1: FP32 SIMT GEMM")
+    ap.add_argument("--probe-mode", type=int, default=None,
+                    help="0 reference probe, 1 BF16 tensor-core probe, 2 FP8-E4M3 centroid scores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
     ap.add_argument("--sweep", action="store_true",
@@ -258,6 +267,9 @@ def main():
         ix.set_top_level_mode(args.top_mode)
     if args.rotation_mode is not None:
         ix.set_rotation_mode(args.rotation_mode)
+    probe_mode = cfg.get("probe_mode", 0) if args.probe_mode is None else args.probe_mode
+    if probe_mode:
+        ix.set_probe_mode(probe_mode)
     rot_tc = ix.rotation_uses_tensor_cores()
     nq, k, d = cfg["nq"], cfg["k"], cfg["d"]
     Qh = gm.sample(nq, 1 + rank)  # rank-specific batch; the first GT_QUERIES match the GT
@@ -340,11 +352,17 @@ def main():
         times.append(ix.kernel_times())
         flush.zero_()
     torch.cuda.synchronize()
-    kern_ms = statistics.mean(t["scan"] for t in times)
+    kern_ms = statistics.mean(t["search_kernel"] for t in times)
+    start_ms = statistics.mean(t["start"] for t in times)
     top_ms = statistics.mean(t["top_level"] for t in times)
     prep_ms = statistics.mean(t["prepare"] for t in times)
     bp = stats["bytes_by_phase"]
-    scan_bytes = bp["start"] + bp["warmup"] + bp["survivor_horizontal"] + bp["survivor_vertical"] + bp["probe"]
+    batched_start = start_ms > 0.0
+    # index bytes the scan kernel itself reads per the algorithm: warmup rows, survivor rows,
+    # centroids of an in-kernel probe, and for each query's first cluster either its full
+    # vectors (Start in the kernel) or the 4-byte distances the batched Start wrote for it
+    start_reads = (bp["start"] // d) * 4 if batched_start else bp["start"]
+    scan_bytes = bp["warmup"] + bp["survivor_horizontal"] + bp["survivor_vertical"] + bp["probe"] + start_reads
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak = float(json.load(open(peaks_path))["hbm_gbs"])
@@ -356,6 +374,11 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(args.config)
+
+    # ---- probe-set error against the FP64 nearest L1 centroids (probe modes 1 and 2)
+    probe = None
+    if probe_mode and rank == 0:
+        probe = probe_report(ix, path, Qh[:len(gt)], cfg, k, gt, device, sp, probe_mode)
 
     # ---- plain path: one query per launch (p50 / p99 latency)
     lat = []
@@ -444,14 +467,18 @@ def main():
                 "latency_ms_batch": {"p50": round(float(np.percentile(step_ms, 50)), 3),
                                      "p99": round(float(np.percentile(step_ms, 99)), 3)},
                 "parallelism": f"replicas{world}" if world > 1 else "single",
-                "rotation": "tcgen05 TF32x3" if rot_tc else "FP32 SIMT",
+                "rotation": ("tcgen05 BF16" if probe_mode else ("tcgen05 TF32x3" if rot_tc else "FP32 SIMT")),
+                "probe": probe if probe_mode else "reference (exact)",
             },
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": "search_kernel", "kernel_ms": round(kern_ms, 3),
                          "algorithmic_bytes_per_launch": scan_bytes, "peak_source": peak_src,
-                         "other_kernels_ms": {"top_level_kernel": round(top_ms, 3),
-                                              "query_norms + rotation": round(prep_ms, 3)},
+                         "other_kernels_ms": {("precision probe (rotation + scores + select)" if probe_mode
+                                               else "tree top level"): round(top_ms, 3),
+                                              "batched start": round(start_ms, 3),
+                                              "query preparation": round(prep_ms, 3)},
+                         "batched_start_replaces_bytes": bp["start"] if batched_start else 0,
                          "top_level_bytes_l2_resident": bp["top_level"],
                          "clusters_visited": stats["clusters_visited"],
                          "bytes_by_phase": stats["bytes_by_phase"],
@@ -467,6 +494,51 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def probe_report(ix, path, Q, cfg, k, gt, device, stream, restore_mode):
+    """Probe-set mismatch of the reduced-precision probe against the FP64 nearest L1 centroids
+    of the FP64-normalized, FP64-rotated queries, and recall of its results; for probe modes 1
+    (BF16 scores) and 2 (FP8-E4M3 scores). Leaves the index in its original probe mode."""
+    import torch
+    from pdx_b200.layout import read_index
+    f = read_index(open(path, "rb").read())
+    rot = np.asarray(f.rotation, np.float64)
+    if f.l0 is not None:  # tree: the L1 centroids are the meso clusters' vectors
+        C = np.zeros((f.l1.nclusters, f.d), np.float64)
+        for emb, ids in zip(f.l0.embeddings, f.l0.row_ids):
+            C[ids] = emb
+    else:
+        C = np.asarray(f.l1.centroids, np.float64)
+    Qd = Q.astype(np.float64)
+    if cfg["normalize"]:
+        Qd = Qd / np.linalg.norm(Qd, axis=1, keepdims=True)
+    R = torch.from_numpy(Qd @ rot).to(device)
+    Ct = torch.from_numpy(C).to(device)
+    nprobe = cfg["nprobe"]
+    d2 = (R * R).sum(1, keepdim=True) - 2.0 * R @ Ct.T + (Ct * Ct).sum(1)[None, :]
+    truth = torch.topk(d2, nprobe, dim=1, largest=False).indices.cpu().numpy()
+    nq = len(Q)
+    q = torch.from_numpy(np.ascontiguousarray(Q)).to(device)
+    ids = torch.empty((nq, k), dtype=torch.int32, device=device)
+    ds = torch.empty((nq, k), dtype=torch.float32, device=device)
+    cnt = torch.empty(nq, dtype=torch.int32, device=device)
+    out = {"vs": "FP64 nearest L1 centroids", "queries": nq, "widened_list": "ceil(1.1 nprobe)"}
+    for mode, name in ((0, "reference_probe"), (1, "bf16"), (2, "fp8_e4m3")):
+        if mode == 0 and f.l0 is None:
+            continue  # the flat reference probe runs inside the scan kernel: no visit orders
+        ix.set_probe_mode(mode)
+        ix.search_device(q.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(), stream=stream)
+        torch.cuda.synchronize()
+        orders, counts = ix.last_visit_orders(nq, nprobe)
+        miss = 1.0 - float(np.mean([len(set(orders[i, :counts[i]].tolist()) & set(truth[i].tolist())) / nprobe
+                                    for i in range(nq)]))
+        ids_np = ids.cpu().numpy().view(np.uint32)
+        cnt_np = cnt.cpu().numpy().view(np.uint32)
+        out[name] = {"probe_set_mismatch": round(miss, 5), "recall@10": round(recall_at(ids_np, cnt_np, gt, 10), 4),
+                     f"recall@{k}": round(recall_at(ids_np, cnt_np, gt, k), 4)}
+    ix.set_probe_mode(restore_mode)
+    return out
 
 
 def run_serve(args, cfg, path, gm, gt, rank, world, local_rank):

@@ -145,6 +145,9 @@ uint32_t pdxg_last_launch_count(const pdxg_index* index);
  * kernel (0 for a stage that did not run). Waits for that search to finish. No counterpart in
  * the reference; used for the roofline accounting. */
 int pdxg_kernel_times(pdxg_index* index, float out[3]);
+/* As pdxg_kernel_times, split finer: out[0] query preparation, out[1] tree top level or the
+ * reduced-precision probe, out[2] the batched Start, out[3] the scan kernel (n >= 4). */
+int pdxg_kernel_times_ex(pdxg_index* index, float* out, uint32_t n);
 
 /* Size of the fixed scratch array behind pdxg_search_device_noalloc, per GPU. */
 #define PDXG_NOALLOC_SCRATCH_BYTES (8u << 20)

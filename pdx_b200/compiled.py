@@ -57,6 +57,7 @@ def library() -> C.CDLL:
         fn("pdxg_last_launch_count", C.c_uint32, vp)
         fn("pdxg_set_start_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_probe_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_kernel_times_ex", C.c_int, vp, vp, C.c_uint32)
         fn("pdxg_last_visit_orders", C.c_int, vp, C.c_uint32, C.c_uint32, vp, vp)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_search_device", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp)
@@ -315,10 +316,13 @@ class PDXIndex:
         return int(library().pdxg_last_launch_count(self._handle().ptr))
 
     def kernel_times(self) -> dict:
-        """Durations (ms) of the last search_device(..., time_kernels=True)."""
-        out = np.zeros(3, np.float32)
-        _check(library().pdxg_kernel_times(self._handle().ptr, out))
-        return {"prepare": float(out[0]), "top_level": float(out[1]), "scan": float(out[2])}
+        """Durations (ms) of the last search_device(..., time_kernels=True): query preparation,
+        tree top level or reduced-precision probe, batched Start, scan kernel ("scan" is the
+        batched Start plus the scan kernel)."""
+        out = np.zeros(4, np.float32)
+        _check(library().pdxg_kernel_times_ex(self._handle().ptr, out.ctypes.data, 4))
+        return {"prepare": float(out[0]), "top_level": float(out[1]), "start": float(out[2]),
+                "search_kernel": float(out[3]), "scan": float(out[2] + out[3])}
 
     def set_pruning_aggressiveness(self, epsilon0: float) -> None:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))

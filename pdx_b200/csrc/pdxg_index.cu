@@ -370,7 +370,9 @@ struct pdxg_index {
     std::vector<uint32_t> rid_cluster, rid_pos;
     cudaStream_t stream = nullptr;
     cudaStream_t stats_stream = nullptr;
-    cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // PDXG_TIME_KERNELS marks
+    // PDXG_TIME_KERNELS marks: start, after preparation, after top level / probe, after the
+    // batched Start, end
+    cudaEvent_t tev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool tev_ready = false, tev_top = false, tev_prep = false;
     uint32_t last_launches = 0;  // engine kernels launched by the last search_device_impl
     uint32_t last_order_stride = 0;  // row stride of the visit orders of the last search (0: none)
@@ -1215,9 +1217,10 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     launches += L.start_launches;
     ix->last_launches = launches;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
+    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     if (timed) {
-        PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
+        PDXG_CUDA(cudaEventRecord(ix->tev[4], st));
         ix->tev_ready = true;
     }
     return PDXG_OK;
@@ -1550,19 +1553,27 @@ int pdxg_rotation_uses_tensor_cores(const pdxg_index* ix) { return ix && ix->rot
 uint32_t pdxg_last_launch_count(const pdxg_index* ix) { return ix ? ix->last_launches : 0; }
 
 int pdxg_kernel_times(pdxg_index* ix, float out[3]) {
+    float t[4];
+    if (int rc = pdxg_kernel_times_ex(ix, t, 4)) return rc;
+    out[0] = t[0];
+    out[1] = t[1];
+    out[2] = t[2] + t[3];
+    return PDXG_OK;
+}
+
+int pdxg_kernel_times_ex(pdxg_index* ix, float* out, uint32_t n) {
     if (int rc = check_index(ix)) return rc;
-    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (!out || n < 4) return fail(PDXG_ERR_INVALID_ARGUMENT, "out must hold 4 values");
     std::lock_guard<std::mutex> lock(ix->mu);
     if (!ix->tev_ready) return fail(PDXG_ERR_INVALID_ARGUMENT, "no search ran with PDXG_TIME_KERNELS");
     PDXG_CUDA(cudaSetDevice(ix->device));
-    PDXG_CUDA(cudaEventSynchronize(ix->tev[3]));
-    float a = 0.0f, b = 0.0f, c = 0.0f;
-    PDXG_CUDA(cudaEventElapsedTime(&a, ix->tev[0], ix->tev[1]));
-    PDXG_CUDA(cudaEventElapsedTime(&b, ix->tev[1], ix->tev[2]));
-    PDXG_CUDA(cudaEventElapsedTime(&c, ix->tev[2], ix->tev[3]));
-    out[0] = ix->tev_prep ? a : 0.0f;
-    out[1] = ix->tev_top ? b : 0.0f;
-    out[2] = c;
+    PDXG_CUDA(cudaEventSynchronize(ix->tev[4]));
+    float t[4];
+    for (int i = 0; i < 4; ++i) PDXG_CUDA(cudaEventElapsedTime(&t[i], ix->tev[i], ix->tev[i + 1]));
+    out[0] = ix->tev_prep ? t[0] : 0.0f;
+    out[1] = ix->tev_top ? t[1] : 0.0f;
+    out[2] = t[2];
+    out[3] = t[3];
     return PDXG_OK;
 }
 
