@@ -369,6 +369,8 @@ struct pdxg_index {
     size_t max_smem = 0;
     std::vector<uint32_t> rid_cluster, rid_pos;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host-buffer search: query upload of later chunks
+    cudaEvent_t chunk_ev[8] = {};
     cudaStream_t stats_stream = nullptr;
     // PDXG_TIME_KERNELS marks: start, after preparation, after top level / probe, after the
     // batched Start, end
@@ -455,6 +457,9 @@ void free_index(pdxg_index* ix) {
         if (e) cudaEventDestroy(e);
     free_workspace(ix->ws);
     if (ix->stream) cudaStreamDestroy(ix->stream);
+    if (ix->copy_stream) cudaStreamDestroy(ix->copy_stream);
+    for (cudaEvent_t e : ix->chunk_ev)
+        if (e) cudaEventDestroy(e);
     delete ix;
 }
 
@@ -826,7 +831,8 @@ uint32_t warmup_checkpoints(uint32_t dv, uint32_t* cp, uint32_t cap) {
 // Tiled top level (pdxg_toplevel.cu). Returns PDXG_OK with L.p.q_order set when it ran,
 // PDXG_OK with L.p.q_order unset when this index or batch does not fit its limits (the caller
 // then uses the per-query form), or an error.
-int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
+                        uint32_t q_offset = 0) {
     const DevLevel& l0 = L.p.l0;
     const HostLevel& h0 = ix->l0;
     if (l0.d % 4 || l0.dv % 4 || l0.dv == 0 || ((uintptr_t)qp & 15) || h0.fc.empty()) return PDXG_OK;
@@ -873,8 +879,8 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
     if ((rc = dev_grow(w.d_top_lists, w.top_lists_cap, (uint64_t)nL0 * nq))) return rc;
     if ((rc = dev_grow(w.d_top_count, w.top_count_cap, (uint64_t)nL0 + nq))) return rc;
     if ((rc = dev_grow(w.d_top_vals, w.top_vals_cap, std::max<uint64_t>((uint64_t)nq * per_query, 4)))) return rc;
-    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
-    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)(q_offset + nq) * k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, q_offset + nq))) return rc;
     tp.arena = ix->arena;
     tp.l0 = l0;
     tp.ratios = L.p.ratios;
@@ -892,8 +898,8 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
     tp.lists = w.d_top_lists;
     tp.vals = w.d_top_vals;
     tp.per_query = per_query;
-    tp.l1_order = w.d_l1_order;
-    tp.l1_count = w.d_l1_count;
+    tp.l1_order = w.d_l1_order + (uint64_t)q_offset * k1;
+    tp.l1_count = w.d_l1_count + q_offset;
     tp.stats = L.p.stats;
     const uint32_t vtiles = (max_n0 + 31) / 32;
     tp.r_smem = (uint32_t)(ratio_bytes + (uint64_t)warps * wb);
@@ -909,12 +915,13 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
 // small per-query CTAs (top_level_kernel; mode 2, and mode 0 otherwise). On success the search
 // kernel reads each query's L1 order from L.p.q_order; in mode 1 the search kernel runs the
 // top level itself.
-int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
+                  uint32_t q_offset = 0) {
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
     if (ix->top_mode == 1) return PDXG_OK;
     if (ix->top_mode == 0 || ix->top_mode == 3) {
-        int rc = run_top_level_tiled(ix, w, qp, nq, L, st);
+        int rc = run_top_level_tiled(ix, w, qp, nq, L, st, q_offset);
         if (rc || L.p.q_order) return rc;
         if (ix->top_mode == 3)
             return fail(PDXG_ERR_CAPACITY, "tiled top level cannot run on this index or batch "
@@ -950,10 +957,10 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
         return PDXG_OK;
     }
     int rc;
-    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
-    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
-    tp.q_order = w.d_l1_order;
-    tp.q_order_count = w.d_l1_count;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)(q_offset + nq) * k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, q_offset + nq))) return rc;
+    tp.q_order = w.d_l1_order + (uint64_t)q_offset * k1;
+    tp.q_order_count = w.d_l1_count + q_offset;
     tp.q_order_stride = k1;
     tp.queue = w.d_queue + 2;
     PDXG_CUDA(cudaMemsetAsync(tp.queue, 0, sizeof(uint32_t), st));
@@ -1270,6 +1277,78 @@ int check_index(const pdxg_index* ix) {
 }
 
 // Host-buffer search shared by pdxg_search / _with_order / filtered variants.
+// Host-buffer search of a plain batch (no order, no filter) with the query upload pipelined:
+// the batch goes up in chunks on a copy stream, each chunk is rotated and runs its tree top
+// level on the compute stream while the next chunk uploads; the batched Start and the scan then
+// run once over the whole batch (their cross-query reuse grows with the batch).
+constexpr uint32_t kPipelineMinQueries = 4096;
+
+int search_host_pipelined(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
+                          uint32_t* ids, float* dists, uint32_t* counts) {
+    Workspace& w = ix->ws;
+    cudaStream_t st = ix->stream;
+    const uint32_t d = ix->d;
+    const bool transformed = (flags & PDXG_QUERY_TRANSFORMED) != 0;
+    int rc;
+    if (!ix->copy_stream) PDXG_CUDA(cudaStreamCreateWithFlags(&ix->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ix->chunk_ev)
+        if (!e) PDXG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    const uint32_t nch = 2;  // measured on B200: 2 chunks beat 4 (the top level loses tile fill)
+    const uint32_t chunk = (nq + nch - 1) / nch;
+    Launch L;
+    if ((rc = plan_search(ix, nq, k, 0, false, L))) return rc;
+    L.p.out_ids = w.d_ids;
+    L.p.out_dists = w.d_dists;
+    L.p.out_counts = w.d_counts;
+    L.p.queue = w.d_queue;
+    const uint32_t k1 = L.p.nprobe;
+    const bool top = ix->tree && ix->top_mode != 1;
+    if (top) {
+        if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
+        if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    }
+    uint32_t launches = 1;
+    bool orders = top;
+    for (uint32_t c = 0; c < nch; ++c) {
+        const uint32_t off = c * chunk;
+        if (off >= nq) break;
+        const uint32_t n = std::min(chunk, nq - off);
+        PDXG_CUDA(cudaMemcpyAsync(w.d_q + (uint64_t)off * d, queries + (uint64_t)off * d, sizeof(float) * n * d,
+                                  cudaMemcpyHostToDevice, ix->copy_stream));
+        PDXG_CUDA(cudaEventRecord(ix->chunk_ev[c], ix->copy_stream));
+        PDXG_CUDA(cudaStreamWaitEvent(st, ix->chunk_ev[c], 0));
+        const float* qc = w.d_q + (uint64_t)off * d;
+        if (!transformed) {
+            if ((rc = prepare_dev(ix, w, qc, n, w.d_rq + (uint64_t)off * d, st))) return rc;
+            qc = w.d_rq + (uint64_t)off * d;
+            launches += (ix->rot_tc && ix->rot_mode == 0) ? 2 : (ix->normalized ? 2 : 1);
+        }
+        if (top) {
+            Launch Lc = L;
+            if ((rc = run_top_level(ix, w, qc, n, Lc, st, off))) return rc;
+            orders = orders && Lc.p.q_order != nullptr;
+            launches += Lc.top_launches;
+        }
+    }
+    L.p.queries = transformed ? w.d_q : w.d_rq;
+    if (orders) {
+        L.p.q_order = w.d_l1_order;
+        L.p.q_order_count = w.d_l1_count;
+        L.p.q_order_stride = k1;
+    }
+    if ((rc = run_start_batched(ix, w, L.p.queries, nq, L, st))) return rc;
+    launches += L.start_launches;
+    ix->last_launches = launches;
+    ix->last_order_stride = L.p.q_order ? k1 : 0;
+    PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
+    PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
+    PDXG_CUDA(cudaMemcpyAsync(ids, w.d_ids, sizeof(uint32_t) * nq * k, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaMemcpyAsync(dists, w.d_dists, sizeof(float) * nq * k, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaMemcpyAsync(counts, w.d_counts, sizeof(uint32_t) * nq, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return check_gemm_error(w);
+}
+
 int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
                      const uint32_t* order, uint32_t n_order,
                      const std::vector<uint32_t>* sel, const std::vector<uint32_t>* pass,
@@ -1282,6 +1361,9 @@ int search_host_impl(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t
     if (rc) return rc;
     Workspace& w = ix->ws;
     cudaStream_t st = ix->stream;
+    if (nq >= kPipelineMinQueries && k > 0 && !(order && n_order) && !(sel && !sel->empty()) &&
+        ix->probe_mode == 0 && !(flags & PDXG_COLLECT_STATS) && !(flags & PDXG_TIME_KERNELS))
+        return search_host_pipelined(ix, queries, nq, k, flags, ids, dists, counts);
     PDXG_CUDA(cudaMemcpyAsync(w.d_q, queries, sizeof(float) * nq * ix->d, cudaMemcpyHostToDevice, st));
     const uint32_t* d_order = nullptr;
     if (order && n_order) {

@@ -360,6 +360,35 @@ def test_batched_start_matches_scan_start(port_cls, top_mode):
         port.close()
 
 
+@pytest.mark.parametrize("itype", ["pdx_tree_u8", "pdx_tree_f32", "pdx_u8"])
+def test_host_pipelined_equals_device_search(itype):
+    """Host-buffer batches of >= 4096 queries upload in chunks overlapped with the per-chunk
+    rotation and top level; results equal the device-buffer search of the whole batch."""
+    import torch
+    gm = GaussianMixture(256, 30, 0.4, seed=17, unit_norm=True)
+    X = gm.sample(6000, 0)
+    Q = gm.sample(5000, 1)
+    nmeso = 8 if "tree" in itype else 0
+    f = build_index(X, itype, num_clusters=60, num_meso_clusters=nmeso, normalize=True, seed=8)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        ix = compiled.load_index(p)
+        ix.set_nprobe(9)
+        k = 10
+        hi, hd, hc = ix.search_batch(Q, k)
+        q = torch.from_numpy(Q).cuda()
+        ids = torch.empty((len(Q), k), dtype=torch.int32, device="cuda")
+        ds = torch.empty((len(Q), k), dtype=torch.float32, device="cuda")
+        cnt = torch.empty(len(Q), dtype=torch.int32, device="cuda")
+        ix.search_device(q.data_ptr(), len(Q), k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(),
+                         stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(hc, cnt.cpu().numpy().view(np.uint32))
+        np.testing.assert_array_equal(hi, ids.cpu().numpy().view(np.uint32))
+        np.testing.assert_array_equal(hd, ds.cpu().numpy())
+
+
 def test_tree_top_level_batched_edge_sizes(port_cls):
     for itype in ("pdx_tree_f32", "pdx_tree_u8"):
         f, X = _manual_index(itype, 200, [0, 1, 31, 33, 0, 5, 64, 257, 2, 0, 90, 7])
