@@ -210,6 +210,8 @@ def main():
     ap.add_argument("--probe-mode", type=int, default=None,
                     help="0 reference probe, 1 BF16 tensor-core probe, 2 FP8-E4M3 centroid scores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default forms")
+    ap.add_argument("--no-graph", action="store_true", help="launch each step directly, not from a CUDA graph")
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
     ap.add_argument("--sweep", action="store_true",
                     help="print recall@10 / QPS over an nprobe ladder and exit")
@@ -284,9 +286,19 @@ def main():
     cnt_dev = torch.empty(nq, dtype=torch.int32, device=device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)  # > 126 MB L2
 
+    tuned = None
+    if not args.no_autotune and not args.sweep and args.threads == 0 and args.top_mode is None:
+        tuned = ix.autotune(q_dev.data_ptr(), nq, k)
+    graph = None
+    if not args.no_graph and not args.sweep:
+        graph = ix.capture(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(), cnt_dev.data_ptr())
+
     def step():
-        ix.search_device(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
-                         cnt_dev.data_ptr(), stream=sp)
+        if graph is not None:
+            graph.launch(sp)
+        else:
+            ix.search_device(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
+                             cnt_dev.data_ptr(), stream=sp)
 
     if args.sweep:
         gq = torch.from_numpy(Qh[:len(gt)]).to(device)
@@ -310,6 +322,10 @@ def main():
         step()
         flush.zero_()
     torch.cuda.synchronize()
+    if graph is not None:  # the graph replays the launches of its capture run
+        ix.search_device(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
+                         cnt_dev.data_ptr(), stream=sp)
+        torch.cuda.synchronize()
     launches_per_step = ix.last_launch_count()
     # quality of this batch's results (rank 0's batch carries the ground-truth queries)
     ids_np = ids_dev.cpu().numpy().view(np.uint32)
@@ -469,6 +485,8 @@ def main():
                 "parallelism": f"replicas{world}" if world > 1 else "single",
                 "rotation": ("tcgen05 BF16" if probe_mode else ("tcgen05 TF32x3" if rot_tc else "FP32 SIMT")),
                 "probe": probe if probe_mode else "reference (exact)",
+                "autotuned": tuned if tuned else "off",
+                "step_launch": "CUDA graph" if graph is not None else "direct",
             },
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -57,6 +57,10 @@ def library() -> C.CDLL:
         fn("pdxg_last_launch_count", C.c_uint32, vp)
         fn("pdxg_set_start_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_probe_mode", C.c_int, vp, C.c_uint32)
+        fn("pdxg_graph_create", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, C.POINTER(vp))
+        fn("pdxg_graph_launch", C.c_int, vp, vp)
+        fn("pdxg_graph_free", None, vp)
+        fn("pdxg_autotune", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp)
         fn("pdxg_kernel_times_ex", C.c_int, vp, vp, C.c_uint32)
         fn("pdxg_last_visit_orders", C.c_int, vp, C.c_uint32, C.c_uint32, vp, vp)
         fn("pdxg_search", C.c_int, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp)
@@ -97,6 +101,22 @@ def _check(rc: int) -> None:
         if rc == PDXG_ERR_INVALID_ARGUMENT:
             raise ValueError(msg)
         raise RuntimeError(msg)
+
+
+class SearchGraph:
+    """A captured device search; launch() replays it on a stream."""
+
+    def __init__(self, ptr, owner):
+        self.ptr = ptr
+        self._owner = owner  # the index outlives the graph
+
+    def launch(self, stream: int = 0) -> None:
+        _check(library().pdxg_graph_launch(self.ptr, C.c_void_p(stream)))
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and self.ptr.value:
+            library().pdxg_graph_free(self.ptr)
+            self.ptr = C.c_void_p()
 
 
 class Handle:
@@ -335,6 +355,22 @@ class PDXIndex:
     def set_start_mode(self, mode: int) -> None:
         """U8 tree indexes: 0 batched first-cluster Start when it fits, 1 inside the scan."""
         _check(library().pdxg_set_start_mode(self._handle().ptr, int(mode)))
+
+    def autotune(self, queries_ptr: int, nq: int, knn: int, transformed: bool = False) -> dict:
+        """Times the engine's forms on this batch of device queries and keeps the fastest."""
+        out = np.zeros(3, np.uint32)
+        _check(library().pdxg_autotune(self._handle().ptr, C.c_void_p(queries_ptr), nq, knn,
+                                       PDXG_QUERY_TRANSFORMED if transformed else 0, out.ctypes.data))
+        return {"threads_per_query": int(out[0]), "top_level_mode": int(out[1]), "start_mode": int(out[2])}
+
+    def capture(self, queries_ptr: int, nq: int, knn: int, ids_ptr: int, dists_ptr: int, counts_ptr: int,
+                transformed: bool = False) -> "SearchGraph":
+        """CUDA graph of one device search of this batch (see pdxg_graph_create)."""
+        g = C.c_void_p()
+        _check(library().pdxg_graph_create(self._handle().ptr, C.c_void_p(queries_ptr), nq, knn,
+                                           PDXG_QUERY_TRANSFORMED if transformed else 0, C.c_void_p(ids_ptr),
+                                           C.c_void_p(dists_ptr), C.c_void_p(counts_ptr), C.byref(g)))
+        return SearchGraph(g, self)
 
     def set_probe_mode(self, mode: int) -> None:
         """0 reference probe; 1 BF16 tensor-core rotation + centroid scores, widened list, FP32

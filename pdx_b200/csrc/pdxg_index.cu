@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <atomic>
 #include <functional>
 #include <mutex>
 #include <string>
@@ -391,9 +392,14 @@ struct pdxg_index {
 
 namespace {
 
+// Incremented whenever a device buffer is replaced: a captured search graph holds raw buffer
+// pointers and refuses to launch once any of them may have moved.
+std::atomic<uint64_t> g_alloc_gen{0};
+
 template <class T>
 int dev_grow(T*& ptr, uint64_t& cap, uint64_t need) {
     if (need <= cap && ptr) return PDXG_OK;
+    g_alloc_gen.fetch_add(1);
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     cap = 0;
@@ -1532,6 +1538,141 @@ int pdxg_search_device(pdxg_index* ix, const float* queries, uint32_t nq, uint32
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ix->stream;
     return search_device_impl(ix, ix->ws, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr,
                               false, ids, distances, counts, st);
+}
+
+}  // extern "C"
+
+struct pdxg_graph {
+    pdxg_index* ix = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;  // g_alloc_gen at capture
+};
+
+extern "C" {
+
+int pdxg_graph_create(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags,
+                      uint32_t* ids, float* distances, uint32_t* counts, pdxg_graph** out) {
+    if (int rc = check_index(ix)) return rc;
+    if (!queries || !ids || !distances || !counts || !out) return fail(PDXG_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (flags & (PDXG_COLLECT_STATS | PDXG_TIME_KERNELS))
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "statistics and kernel timing are not captured in a graph");
+    if (nq == 0 || k == 0) return fail(PDXG_ERR_INVALID_ARGUMENT, "empty batch");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    // a direct run sizes every workspace buffer for this batch, so the capture allocates nothing
+    int rc = search_device_impl(ix, ix->ws, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr, false,
+                                ids, distances, counts, ix->stream);
+    if (rc) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(ix->stream));
+    if ((rc = check_gemm_error(ix->ws))) return rc;
+    const uint64_t gen = g_alloc_gen.load();
+    cudaStream_t cs = nullptr;
+    PDXG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = search_device_impl(ix, ix->ws, queries, nq, k, flags, nullptr, 0, nullptr, nullptr, nullptr, false,
+                                ids, distances, counts, cs);
+        e = cudaStreamEndCapture(cs, &graph);
+    }
+    cudaStreamDestroy(cs);
+    if (rc == PDXG_OK && (e != cudaSuccess || g_alloc_gen.load() != gen))
+        rc = fail(PDXG_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    if (rc == PDXG_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        rc = fail(PDXG_ERR_CUDA, "graph instantiation failed");
+    if (rc != PDXG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    pdxg_graph* g = new pdxg_graph();
+    g->ix = ix;
+    g->graph = graph;
+    g->exec = exec;
+    g->gen = gen;
+    *out = g;
+    return PDXG_OK;
+}
+
+int pdxg_graph_launch(pdxg_graph* g, void* stream) {
+    if (!g) return fail(PDXG_ERR_INVALID_ARGUMENT, "graph is NULL");
+    if (g_alloc_gen.load() != g->gen)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "the engine's buffers changed since the capture; create the graph again");
+    PDXG_CUDA(cudaSetDevice(g->ix->device));
+    PDXG_CUDA(cudaGraphLaunch(g->exec, stream ? static_cast<cudaStream_t>(stream) : g->ix->stream));
+    return PDXG_OK;
+}
+
+void pdxg_graph_free(pdxg_graph* g) {
+    if (!g) return;
+    cudaSetDevice(g->ix->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
+int pdxg_autotune(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k, uint32_t flags, uint32_t choice[3]) {
+    if (int rc = check_index(ix)) return rc;
+    if (!queries || !choice || nq == 0 || k == 0) return fail(PDXG_ERR_INVALID_ARGUMENT, "bad arguments");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    flags &= ~(uint32_t)(PDXG_COLLECT_STATS | PDXG_TIME_KERNELS);
+    uint32_t *ids = nullptr, *counts = nullptr;
+    float* dists = nullptr;
+    int rc = PDXG_OK;
+    if (cudaMalloc(&ids, (size_t)nq * k * 4) != cudaSuccess || cudaMalloc(&dists, (size_t)nq * k * 4) != cudaSuccess ||
+        cudaMalloc(&counts, (size_t)nq * 4) != cudaSuccess)
+        rc = fail(PDXG_ERR_CUDA, "cannot allocate the tuning outputs");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == PDXG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = fail(PDXG_ERR_CUDA, "cannot create events");
+    const uint32_t old_threads = ix->threads, old_top = ix->top_mode, old_start = ix->start_mode;
+    const uint32_t threads_c[3] = {64, 128, 256};
+    const uint32_t tops_c[2] = {3, 2};
+    const uint32_t starts_c[2] = {0, 1};
+    const uint32_t ntop = ix->tree ? 2 : 1, nstart = (ix->tree && ix->u8) ? 2 : 1;
+    float best = 1e30f;
+    uint32_t bt = old_threads, btop = old_top, bstart = old_start;
+    for (uint32_t a = 0; a < 3 && rc == PDXG_OK; ++a)
+        for (uint32_t b = 0; b < ntop && rc == PDXG_OK; ++b)
+            for (uint32_t c = 0; c < nstart && rc == PDXG_OK; ++c) {
+                ix->threads = threads_c[a];
+                ix->top_mode = ix->tree ? tops_c[b] : old_top;
+                ix->start_mode = starts_c[c];
+                float t_min = 1e30f;
+                for (int rep = 0; rep < 4 && rc == PDXG_OK; ++rep) {
+                    if (cudaEventRecord(e0, ix->stream) != cudaSuccess) rc = fail(PDXG_ERR_CUDA, "event");
+                    if (rc == PDXG_OK)
+                        rc = search_device_impl(ix, ix->ws, queries, nq, k, flags, nullptr, 0, nullptr, nullptr,
+                                                nullptr, false, ids, dists, counts, ix->stream);
+                    if (rc == PDXG_OK && (cudaEventRecord(e1, ix->stream) != cudaSuccess ||
+                                          cudaEventSynchronize(e1) != cudaSuccess))
+                        rc = fail(PDXG_ERR_CUDA, "event");
+                    float ms = 0.0f;
+                    if (rc == PDXG_OK && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+                        t_min = std::min(t_min, ms);  // the first run of a form warms it up
+                }
+                if (rc == PDXG_OK && t_min < best) {
+                    best = t_min;
+                    bt = ix->threads;
+                    btop = ix->top_mode;
+                    bstart = ix->start_mode;
+                }
+            }
+    if (rc == PDXG_OK) rc = check_gemm_error(ix->ws);
+    ix->threads = rc == PDXG_OK ? bt : old_threads;
+    ix->top_mode = rc == PDXG_OK ? btop : old_top;
+    ix->start_mode = rc == PDXG_OK ? bstart : old_start;
+    choice[0] = ix->threads;
+    choice[1] = ix->top_mode;
+    choice[2] = ix->start_mode;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(ids);
+    cudaFree(dists);
+    cudaFree(counts);
+    return rc;
 }
 
 int pdxg_search_with_order(pdxg_index* ix, const float* queries, uint32_t nq, uint32_t k,
