@@ -34,6 +34,7 @@ cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t s
 cudaError_t launch_row_sq(const float* x, uint32_t n, uint32_t d, float* out, cudaStream_t st);
 size_t probe_select_smem(uint32_t d, uint32_t n1, uint32_t cand_cap, uint32_t sort_cap);
 cudaError_t launch_probe_select(const ProbeParams& pp, cudaStream_t st);
+cudaError_t launch_probe_exact(const ProbeParams& pp, cudaStream_t st);
 int start_dist_occupancy(size_t smem);
 size_t start_dist_smem(const DevLevel& lv);
 uint64_t start_item_bound(uint32_t nq, uint32_t n1, uint32_t max_n);
@@ -685,7 +686,8 @@ struct Launch {
 };
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
-                Launch& L, uint32_t np_flat_max = 0xFFFFFFFFu, uint32_t top_max = 0xFFFFFFFFu) {
+                Launch& L, uint32_t np_flat_max = 0xFFFFFFFFu, uint32_t top_max = 0xFFFFFFFFu,
+                bool probe_ahead = false) {
     SearchParams& p = L.p;
     p.arena = ix->arena;
     p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale);
@@ -710,15 +712,18 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
     p.top_nprobe = top;
     p.n_order = n_order;
     const uint32_t d = ix->d;
-    // the heap region also holds the sorted probe list (flat: nprobe, tree L0: top entries)
-    const uint32_t heap_cap = next_pow2(std::max({k, np_flat, top, 1u}));
+    // the heap region also holds the sorted probe list of an in-kernel probe (flat: nprobe,
+    // tree L0: top entries); orders computed ahead are read in place
+    const uint32_t heap_cap = probe_ahead ? next_pow2(std::max(k, 1u)) : next_pow2(std::max({k, np_flat, top, 1u}));
     uint32_t work = std::max({p.l1.max_n, heap_cap, 32u});
-    if (!ix->tree || any_filter) work = std::max(work, n1);
+    // an in-kernel probe keeps one entry per centroid (not needed when the visit orders are
+    // computed ahead of the scan)
+    if ((!ix->tree && !probe_ahead) || any_filter) work = std::max(work, n1);
     if (ix->tree) work = std::max({work, p.l0.max_n, p.l0.nclusters});
     // dist/pos need max cluster size (or centroid count for a probe); sorts viewing the region as
     // u64 need at most heap_cap (a power of two) entries, so no power-of-two padding here
     const uint32_t work_cap = (work + 31) / 32 * 32;
-    const uint32_t order_cap = std::max({np_flat, top, n_order, 1u});
+    const uint32_t order_cap = probe_ahead ? std::max(n_order, 1u) : std::max({np_flat, top, n_order, 1u});
     uint32_t off = 0;
     p.smem_qf = off;
     off += (uint32_t)align_up((uint64_t)d * 4, 16);
@@ -1111,6 +1116,42 @@ int run_probe_gemm(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, bo
     return PDXG_OK;
 }
 
+// Exact probe of a flat index ahead of the scan (probe_exact_kernel): same order as the scan
+// kernel's own probe; lets the scan keep per-vector arrays only.
+constexpr uint32_t kProbeAheadMinQueries = 32;
+
+bool probe_exact_ok(const pdxg_index* ix) {
+    const uint32_t n1 = (uint32_t)ix->l1.fc.size();
+    return !ix->tree && probe_select_smem(ix->d, n1, (n1 + 3) & ~3u, next_pow2(n1)) + 2048 <= ix->max_smem;
+}
+
+int run_probe_exact(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st) {
+    const uint32_t n1 = L.p.l1.nclusters, k1 = L.p.nprobe;
+    int rc;
+    if ((rc = dev_grow(w.d_l1_order, w.l1_order_cap, (uint64_t)nq * k1))) return rc;
+    if ((rc = dev_grow(w.d_l1_count, w.l1_count_cap, nq))) return rc;
+    ProbeParams pp{};
+    pp.queries = qp;
+    pp.centroids = ix->d_cent1;
+    pp.nq = nq;
+    pp.d = ix->d;
+    pp.nclusters = n1;
+    pp.nprobe = k1;
+    pp.q_nprobe = L.p.q_nprobe;
+    pp.order = w.d_l1_order;
+    pp.stride = k1;
+    pp.count = w.d_l1_count;
+    pp.cand_cap = (n1 + 3) & ~3u;
+    pp.sort_cap = next_pow2(n1);
+    pp.stats = L.p.stats;
+    PDXG_CUDA(launch_probe_exact(pp, st));
+    L.probe_launches += 1;
+    L.p.q_order = w.d_l1_order;
+    L.p.q_order_count = w.d_l1_count;
+    L.p.q_order_stride = k1;
+    return PDXG_OK;
+}
+
 // Batched Start (pdxg_start.cu) for U8 levels whose visit orders are known before the scan
 // (tree indexes with a separate top level). Sets L.p.start_* when it ran; a batch outside its
 // limits leaves them unset and the scan runs Start itself.
@@ -1194,7 +1235,9 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     }
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[1], st));
     Launch L;
-    rc = plan_search(ix, nq, k, n_order, any_filter, L);
+    const bool probe_ahead = !gemm_probe && !ix->tree && !any_filter && !d_order && nq >= kProbeAheadMinQueries &&
+                             probe_exact_ok(ix);
+    rc = plan_search(ix, nq, k, n_order, any_filter, L, 0xFFFFFFFFu, 0xFFFFFFFFu, probe_ahead);
     if (rc) return rc;
     L.p.queries = qp;
     L.p.order = d_order;
@@ -1221,6 +1264,10 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         rc = run_top_level(ix, w, qp, nq, L, st);
         if (rc) return rc;
         launches += L.top_launches;
+    } else if (probe_ahead) {
+        rc = run_probe_exact(ix, w, qp, nq, L, st);
+        if (rc) return rc;
+        launches += L.probe_launches;
     }
     ix->tev_top = L.p.q_order != nullptr;
     ix->last_order_stride = L.p.q_order ? L.p.q_order_stride : 0;

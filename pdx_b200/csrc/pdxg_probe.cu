@@ -34,6 +34,11 @@ __global__ void row_sq_kernel(const float* __restrict__ x, uint32_t n, uint32_t 
 
 constexpr int kSelectThreads = 128;
 
+// Shared memory of one probe CTA: query, one key per centroid, candidates, sort keys.
+size_t probe_select_smem(uint32_t d, uint32_t n1, uint32_t cand_cap, uint32_t sort_cap) {
+    return ((size_t)d * 4 + 15) / 16 * 16 + (size_t)((n1 + 3) & ~3u) * 4 + (size_t)cand_cap * 4 + (size_t)sort_cap * 8;
+}
+
 // Order-preserving map of a float onto uint32 (negative scores included).
 __device__ __forceinline__ uint32_t float_key(float f) {
     const uint32_t b = __float_as_uint(f);
@@ -93,15 +98,68 @@ __global__ void __launch_bounds__(kSelectThreads) probe_select_kernel(const __gr
     }
 }
 
+// Exact probe of a flat index for a whole batch, ahead of the scan (LevelOps::probe's result,
+// searcher.hpp:181-215): FP32 distances to every centroid in the AVX2 Horizontal order, the
+// nprobe nearest by (distance, id), ascending. One CTA per query. The scan kernel then needs no
+// per-centroid arrays in shared memory, only per-vector ones.
+__global__ void __launch_bounds__(kSelectThreads) probe_exact_kernel(const __grid_constant__ ProbeParams pp) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ Scalars s;
+    const uint32_t q = blockIdx.x;
+    const uint32_t n1 = pp.nclusters, d = pp.d;
+    float* qf = reinterpret_cast<float*>(smem);                                         // [d]
+    uint32_t* keys = reinterpret_cast<uint32_t*>(smem + ((size_t)d * 4 + 15) / 16 * 16);  // [n1]
+    uint32_t* cand = keys + ((n1 + 3) & ~3u);                                            // [cand_cap]
+    uint64_t* sortb = reinterpret_cast<uint64_t*>(cand + pp.cand_cap);                   // [sort_cap]
+    const uint32_t np = pp.q_nprobe ? __ldg(pp.q_nprobe + q) : pp.nprobe;
+    const uint32_t m = np < n1 ? np : n1;
+    const float* src = pp.queries + (size_t)q * d;
+    for (uint32_t i = threadIdx.x; i < d; i += kSelectThreads) qf[i] = __ldg(src + i);
+    __syncthreads();
+    const uint32_t sub = threadIdx.x & 7;
+    for (uint32_t base = 0; base < n1; base += kSelectThreads / 8) {
+        const uint32_t c = base + (threadIdx.x >> 3);
+        const bool active = c < n1;
+        const float dd = horiz_f32_group8(qf, pp.centroids + (size_t)(active ? c : 0) * d, d, sub, active);
+        if (active && sub == 0) keys[c] = __float_as_uint(dd);
+    }
+    __syncthreads();
+    uint32_t kth, less;
+    block_radix_select<kSelectThreads>(keys, n1, m, s, kth, less);
+    const uint32_t nl = block_compact<kSelectThreads>(
+        n1, [&](uint32_t, uint32_t v) { return keys[v] < kth; }, [](uint32_t i) { return i; }, cand, s);
+    block_compact<kSelectThreads>(n1, [&](uint32_t, uint32_t v) { return keys[v] == kth; },
+                                  [](uint32_t i) { return i; }, cand + nl, s);
+    const uint32_t N = next_pow2(m);
+    for (uint32_t i = threadIdx.x; i < N; i += kSelectThreads)
+        sortb[i] = (i < m) ? (((uint64_t)keys[cand[i]] << 32) | cand[i]) : ~0ull;
+    __syncthreads();
+    block_bitonic_sort<kSelectThreads>(sortb, N);
+    for (uint32_t i = threadIdx.x; i < m; i += kSelectThreads) pp.order[(size_t)q * pp.stride + i] = (uint32_t)sortb[i];
+    if (threadIdx.x == 0) {
+        pp.count[q] = m;
+        if (pp.stats) {
+            const unsigned long long b = (unsigned long long)n1 * d * 4u;
+            atomicAdd(pp.stats + 8, b);
+            atomicAdd(pp.stats, b);
+        }
+    }
+}
+
+cudaError_t launch_probe_exact(const ProbeParams& pp, cudaStream_t st) {
+    const size_t smem = probe_select_smem(pp.d, pp.nclusters, pp.cand_cap, pp.sort_cap);
+    cudaError_t e = cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    probe_exact_kernel<<<pp.nq, kSelectThreads, smem, st>>>(pp);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_row_sq(const float* x, uint32_t n, uint32_t d, float* out, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     row_sq_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(x, n, d, out);
     return cudaGetLastError();
 }
 
-size_t probe_select_smem(uint32_t d, uint32_t n1, uint32_t cand_cap, uint32_t sort_cap) {
-    return ((size_t)d * 4 + 15) / 16 * 16 + (size_t)((n1 + 3) & ~3u) * 4 + (size_t)cand_cap * 4 + (size_t)sort_cap * 8;
-}
 
 cudaError_t launch_probe_select(const ProbeParams& pp, cudaStream_t st) {
     const size_t smem = probe_select_smem(pp.d, pp.nclusters, pp.cand_cap, pp.sort_cap);

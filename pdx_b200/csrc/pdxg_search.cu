@@ -666,7 +666,9 @@ struct LevelOps {
     }
 
     // Visits clusters order[0, nvisit) (searcher.hpp:655-721 / 776-853).
-    __device__ void run(uint32_t k, uint32_t nvisit) {
+    // `order` is sh.order or, for visit orders computed ahead of the scan, the query's row of
+    // them in global memory.
+    __device__ void run(uint32_t k, uint32_t nvisit, const uint32_t* order) {
         if (threadIdx.x == 0) {
             s.hsize = 0;
             s.top = 0.0f;
@@ -674,7 +676,7 @@ struct LevelOps {
         }
         __syncthreads();
         for (uint32_t ci = 0; ci < nvisit; ++ci) {
-            const uint32_t cidx = sh.order[ci];
+            const uint32_t cidx = order[ci];
             const DevCluster c = lv.clusters[cidx];
             uint32_t passing = 0;
             if (fsel) {
@@ -806,25 +808,24 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
         const uint32_t npq = p.q_nprobe ? __ldg(p.q_nprobe + q) : p.nprobe;
         const uint32_t topq = p.q_top ? __ldg(p.q_top + q) : p.top_nprobe;
         uint32_t nvisit;
+        const uint32_t* visit = sh.order;  // the query's L1 visit order
         if (p.order) {
             // caller-provided access order (PDXearch::SetClusterAccessOrder, searcher.hpp:48-54)
             nvisit = npq < p.n_order ? npq : p.n_order;
             for (uint32_t i = threadIdx.x; i < nvisit; i += T) sh.order[i] = __ldg(p.order + i);
             __syncthreads();
         } else if (filter == -1 && p.q_order) {
-            // the tree top level (pdxg_toplevel.cu) or the reduced-precision probe
-            // (pdxg_probe.cu) already produced this query's L1 order
+            // the tree top level (pdxg_toplevel.cu) or a probe ahead of the scan (pdxg_probe.cu)
+            // already produced this query's L1 order: read in place
             nvisit = __ldg(p.q_order_count + q);
-            for (uint32_t i = threadIdx.x; i < nvisit; i += T)
-                sh.order[i] = __ldg(p.q_order + (size_t)q * p.q_order_stride + i);
-            __syncthreads();
+            visit = p.q_order + (size_t)q * p.q_order_stride;
         } else if (p.is_tree && filter == -1) {
             // PDXTreeIndex::Search (index.hpp:545-566): pruned F32 search over the meso
             // clusters with k = nprobe returns the L1 clusters to visit, nearest first.
             LevelOps<T, false> top(p, p.l0, sh, s, -1, true);
             const uint32_t nv0 = topq < p.l0.nclusters ? topq : p.l0.nclusters;
             top.probe(topq);
-            top.run(npq, nv0);
+            top.run(npq, nv0, sh.order);
             const uint32_t cnt = top.sort_heap(npq);
             for (uint32_t i = threadIdx.x; i < cnt; i += T) sh.order[i] = (uint32_t)sh.sortw[i];
             __syncthreads();
@@ -844,7 +845,7 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             ops.pre_row = __ldg(p.start_row + q);
             ops.pre_cluster = __ldg(p.start_first + q);
         }
-        ops.run(kq, nvisit);
+        ops.run(kq, nvisit, visit);
         const uint32_t cnt = ops.sort_heap(kq);
         uint32_t* oi = p.out_ids + (size_t)q * p.k;
         float* od = p.out_dists + (size_t)q * p.k;
@@ -924,7 +925,7 @@ __global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ Se
         const uint32_t topq = p.q_top ? __ldg(p.q_top + q) : p.top_nprobe;
         const uint32_t nv0 = topq < p.l0.nclusters ? topq : p.l0.nclusters;
         top.probe(topq);
-        top.run(npq, nv0);
+        top.run(npq, nv0, sh.order);
         const uint32_t cnt = top.sort_heap(npq);
         for (uint32_t i = threadIdx.x; i < cnt; i += T)
             out_order[(size_t)q * p.q_order_stride + i] = (uint32_t)sh.sortw[i];

@@ -360,6 +360,17 @@ def test_batched_start_matches_scan_start(port_cls, top_mode):
         port.close()
 
 
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8"])
+def test_flat_probe_ahead_matches_port(port_cls, itype):
+    """Batches of >= 32 queries on flat indexes probe ahead of the scan (probe_exact_kernel);
+    the visit order and the results are the oracle's."""
+    gm = GaussianMixture(192, 25, 0.4, seed=23, unit_norm=True)
+    X = gm.sample(5000, 0)
+    Q = gm.sample(64, 1)
+    f = build_index(X, itype, num_clusters=70, normalize=True, seed=12)
+    _compare_with_port(port_cls, f, Q, 10, (0, 3, 17), threads=(64, 128))
+
+
 @pytest.mark.parametrize("itype", ["pdx_tree_u8", "pdx_tree_f32", "pdx_u8"])
 def test_host_pipelined_equals_device_search(itype):
     """Host-buffer batches of >= 4096 queries upload in chunks overlapped with the per-chunk
