@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(kSelectThreads) probe_select_kernel(const __gr
 // searcher.hpp:181-215): FP32 distances to every centroid in the AVX2 Horizontal order, the
 // nprobe nearest by (distance, id), ascending. One CTA per query. The scan kernel then needs no
 // per-centroid arrays in shared memory, only per-vector ones.
-__global__ void __launch_bounds__(kSelectThreads) probe_exact_kernel(const __grid_constant__ ProbeParams pp) {
+template <int T>
+__global__ void __launch_bounds__(T) probe_exact_kernel(const __grid_constant__ ProbeParams pp) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ Scalars s;
     const uint32_t q = blockIdx.x;
@@ -114,28 +115,33 @@ __global__ void __launch_bounds__(kSelectThreads) probe_exact_kernel(const __gri
     const uint32_t np = pp.q_nprobe ? __ldg(pp.q_nprobe + q) : pp.nprobe;
     const uint32_t m = np < n1 ? np : n1;
     const float* src = pp.queries + (size_t)q * d;
-    for (uint32_t i = threadIdx.x; i < d; i += kSelectThreads) qf[i] = __ldg(src + i);
+    for (uint32_t i = threadIdx.x; i < d; i += T) qf[i] = __ldg(src + i);
     __syncthreads();
     const uint32_t sub = threadIdx.x & 7;
-    for (uint32_t base = 0; base < n1; base += kSelectThreads / 8) {
+    for (uint32_t base = 0; base < n1; base += T / 8) {
         const uint32_t c = base + (threadIdx.x >> 3);
         const bool active = c < n1;
         const float dd = horiz_f32_group8(qf, pp.centroids + (size_t)(active ? c : 0) * d, d, sub, active);
         if (active && sub == 0) keys[c] = __float_as_uint(dd);
     }
     __syncthreads();
-    uint32_t kth, less;
-    block_radix_select<kSelectThreads>(keys, n1, m, s, kth, less);
-    const uint32_t nl = block_compact<kSelectThreads>(
-        n1, [&](uint32_t, uint32_t v) { return keys[v] < kth; }, [](uint32_t i) { return i; }, cand, s);
-    block_compact<kSelectThreads>(n1, [&](uint32_t, uint32_t v) { return keys[v] == kth; },
-                                  [](uint32_t i) { return i; }, cand + nl, s);
+    if (m < n1) {
+        uint32_t kth, less;
+        block_radix_select<T>(keys, n1, m, s, kth, less);
+        const uint32_t nl = block_compact<T>(
+            n1, [&](uint32_t, uint32_t v) { return keys[v] < kth; }, [](uint32_t i) { return i; }, cand, s);
+        block_compact<T>(n1, [&](uint32_t, uint32_t v) { return keys[v] == kth; }, [](uint32_t i) { return i; },
+                         cand + nl, s);
+    } else {
+        for (uint32_t i = threadIdx.x; i < n1; i += T) cand[i] = i;  // every centroid: sort them all
+        __syncthreads();
+    }
     const uint32_t N = next_pow2(m);
-    for (uint32_t i = threadIdx.x; i < N; i += kSelectThreads)
+    for (uint32_t i = threadIdx.x; i < N; i += T)
         sortb[i] = (i < m) ? (((uint64_t)keys[cand[i]] << 32) | cand[i]) : ~0ull;
     __syncthreads();
-    block_bitonic_sort<kSelectThreads>(sortb, N);
-    for (uint32_t i = threadIdx.x; i < m; i += kSelectThreads) pp.order[(size_t)q * pp.stride + i] = (uint32_t)sortb[i];
+    block_bitonic_sort<T>(sortb, N);
+    for (uint32_t i = threadIdx.x; i < m; i += T) pp.order[(size_t)q * pp.stride + i] = (uint32_t)sortb[i];
     if (threadIdx.x == 0) {
         pp.count[q] = m;
         if (pp.stats) {
@@ -148,9 +154,17 @@ __global__ void __launch_bounds__(kSelectThreads) probe_exact_kernel(const __gri
 
 cudaError_t launch_probe_exact(const ProbeParams& pp, cudaStream_t st) {
     const size_t smem = probe_select_smem(pp.d, pp.nclusters, pp.cand_cap, pp.sort_cap);
-    cudaError_t e = cudaFuncSetAttribute(probe_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    probe_exact_kernel<<<pp.nq, kSelectThreads, smem, st>>>(pp);
+    // large levels sort thousands of keys per query: more threads per CTA
+    if (pp.nclusters > 2048) {
+        cudaError_t e = cudaFuncSetAttribute(probe_exact_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        probe_exact_kernel<512><<<pp.nq, 512, smem, st>>>(pp);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(probe_exact_kernel<kSelectThreads>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        probe_exact_kernel<kSelectThreads><<<pp.nq, kSelectThreads, smem, st>>>(pp);
+    }
     return cudaGetLastError();
 }
 
