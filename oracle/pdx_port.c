@@ -668,8 +668,24 @@ pindex* pdxport_load_buffer(const uint8_t* buf, size_t size) {
     const int is_u8 = (ix->type == 1 || ix->type == 3);
     ix->is_tree = ix->type >= 2;
     const uint32_t d = hdr[0], dv = hdr[1], dh = hdr[2];
-    if (d == 0 || d > 16384 || dv + dh != d || rows != d || cols != d) goto bad;
+    if (d == 0 || d > 16384 || dv + dh != d || cols != d || (rows != d && rows != 1)) goto bad;
     ix->d = d;
+    if (rows == 1) {
+        /* adsampling.hpp:192-246, FFTW branch: flip the sign of dimension j where the stored
+         * vector is negative, then the orthonormal DCT-II (FFTW_REDFT10 scaled by sqrt(1/(4d))
+         * for output 0 and sqrt(1/(2d)) for the others). As the d x d matrix of y = x M:
+         * M[j][k] = s_j c_k cos(pi (2j + 1) k / (2d)), c_0 = sqrt(1/d), c_k = sqrt(2/d). */
+        float* dense = (float*)malloc(sizeof(float) * (size_t)d * d);
+        for (uint32_t j = 0; j < d; ++j) {
+            const double sj = ix->rotation[j] < 0.0f ? -1.0 : 1.0;
+            for (uint32_t k = 0; k < d; ++k) {
+                const double ck = k == 0 ? sqrt(1.0 / d) : sqrt(2.0 / d);
+                dense[(size_t)j * d + k] = (float)(sj * ck * cos(3.14159265358979323846 * (2.0 * j + 1.0) * k / (2.0 * d)));
+            }
+        }
+        free(ix->rotation);
+        ix->rotation = dense;
+    }
     if (!ix->is_tree) {
         const uint32_t ncl = hdr[3];
         p += 16;

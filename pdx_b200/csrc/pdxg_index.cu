@@ -333,7 +333,8 @@ struct pdxg_index {
     bool tree = false, u8 = false, normalized = false;
     float base = 0.0f, scale = 1.0f;
     uint32_t rot_rows = 0, rot_cols = 0;
-    std::vector<float> rotation;
+    std::vector<float> rotation;       // d x d matrix of y = x M used by the engine
+    std::vector<float> file_rotation;  // as stored in the file (d x d, or 1 x d DCT signs)
     HostLevel l1, l0;
     uint8_t* arena = nullptr;
     uint64_t arena_bytes = 0;
@@ -500,20 +501,34 @@ int load_from_bytes(const uint8_t* buf, uint64_t size, int device, pdxg_index** 
         free_index(ix);
         return fail(PDXG_ERR_FORMAT, "dimension split in file does not match GetPDXDimensionSplit");
     }
-    if (ix->rot_rows == 1 && ix->rot_cols == d) {
-        free_index(ix);
-        return fail(PDXG_ERR_UNSUPPORTED,
-                    "index uses the DCT rotation (1 x d sign vector); not supported by this engine");
-    }
-    if (ix->rot_rows != d || ix->rot_cols != d) {
+    const bool dct = ix->rot_rows == 1 && ix->rot_cols == d;
+    if (!dct && (ix->rot_rows != d || ix->rot_cols != d)) {
         free_index(ix);
         return fail(PDXG_ERR_FORMAT, "rotation matrix shape does not match num_dimensions");
     }
     ix->d = d;
     ix->dv = dv;
     ix->dh = dh;
+    ix->file_rotation.resize((size_t)ix->rot_rows * ix->rot_cols);
+    std::memcpy(ix->file_rotation.data(), rot, ix->file_rotation.size() * 4);
     ix->rotation.resize((size_t)d * d);
-    std::memcpy(ix->rotation.data(), rot, (size_t)d * d * 4);
+    if (dct) {
+        // Files built with the FFTW rotation store a 1 x d sign vector (adsampling.hpp:192-246):
+        // flip dimension j where it is negative, then the orthonormal DCT-II (FFTW_REDFT10 with
+        // output 0 scaled by sqrt(1/(4d)), the others by sqrt(2/(4d))). The engine applies it as
+        // the d x d matrix of y = x M: M[j][k] = s_j c_k cos(pi (2j + 1) k / (2d)), c_0 = sqrt(1/d),
+        // c_k = sqrt(2/d), through the same rotation GEMMs.
+        for (uint32_t j = 0; j < d; ++j) {
+            const double sj = ix->file_rotation[j] < 0.0f ? -1.0 : 1.0;
+            for (uint32_t k = 0; k < d; ++k) {
+                const double ck = k == 0 ? std::sqrt(1.0 / d) : std::sqrt(2.0 / d);
+                ix->rotation[(size_t)j * d + k] =
+                    (float)(sj * ck * std::cos(M_PI * (2.0 * j + 1.0) * k / (2.0 * d)));
+            }
+        }
+    } else {
+        std::memcpy(ix->rotation.data(), rot, (size_t)d * d * 4);
+    }
     for (HostLevel* lv : {&ix->l1, &ix->l0}) {
         lv->d = d;
         lv->dv = dv;
@@ -1890,7 +1905,7 @@ int pdxg_save(pdxg_index* ix, const char* path) {
     out.write(reinterpret_cast<const char*>(&type), 1);
     w32(ix->rot_rows);
     w32(ix->rot_cols);
-    out.write(reinterpret_cast<const char*>(ix->rotation.data()), ix->rotation.size() * 4);
+    out.write(reinterpret_cast<const char*>(ix->file_rotation.data()), ix->file_rotation.size() * 4);
     auto write_level = [&](const HostLevel& lv) {
         for (size_t i = 0; i < lv.meta.size(); ++i) {
             w32(lv.n[i]);

@@ -59,3 +59,30 @@ def assert_same(ids_a, d_a, ids_b, d_b, rtol=0.0, ctx=""):
 
 def recall(found, truth, k):
     return len(set(np.asarray(found)[:k].tolist()) & set(np.asarray(truth)[:k].tolist())) / max(1, min(k, len(truth)))
+
+
+def dct_index(itype, d, n, nlist, nmeso=0, seed=0):
+    """An index whose file stores the FFTW-style rotation: a 1 x d sign vector (flip where
+    negative) followed by the orthonormal DCT-II. The data are rotated with the same transform
+    in float64 (scipy.fft.dct, norm="ortho")."""
+    import scipy.fft
+    from pdx_b200.builder import GaussianMixture, build_index
+    rng = np.random.default_rng(seed)
+    signs = np.where(rng.random(d) < 0.5, -1.0, 1.0).astype(np.float32)
+    # dense form of x -> dct(x * s): rows j of the matrix are the images of the unit vectors
+    dense = scipy.fft.dct(np.diag(signs.astype(np.float64)), type=2, norm="ortho", axis=1).astype(np.float32)
+    gm = GaussianMixture(d, 20, 0.4, seed=seed + 1, unit_norm=True)
+    X = gm.sample(n, 0)
+    Q = gm.sample(64, 1)
+    f = build_index(X, itype, num_clusters=nlist, num_meso_clusters=nmeso, normalize=True, seed=seed,
+                    rotation=dense)
+    f.rotation = signs.reshape(1, d)
+    return f, Q, signs
+
+
+def dct_rotate(Q, signs, normalize=True):
+    import scipy.fft
+    Q = Q.astype(np.float64)
+    if normalize:
+        Q = Q / np.linalg.norm(Q, axis=1, keepdims=True)
+    return scipy.fft.dct(Q * signs.astype(np.float64)[None, :], type=2, norm="ortho", axis=1)

@@ -162,6 +162,37 @@ def test_edge_cluster_sizes(port_cls, itype):
     _compare_with_port(port_cls, f, Q, 500, (0,))  # k larger than the index
 
 
+@pytest.mark.parametrize("itype", ["pdx_u8", "pdx_tree_f32", "pdx_f32"])
+def test_dct_rotation_files(port_cls, itype):
+    """FFTW-built files (1 x d sign vector + orthonormal DCT-II): the engine rotates as the
+    reference's DCT does (FP32 rounding level against scipy's DCT), searches exactly like the
+    oracle on the same prepared queries, and saves the file back byte for byte."""
+    from tests.helpers import dct_index, dct_rotate
+    nmeso = 6 if "tree" in itype else 0
+    f, Q, signs = dct_index(itype, 512, 6000, 40, nmeso, seed=7)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "dct.pdx")
+        f.save(p)
+        ix = compiled.load_index(p)
+        R = ix.prepare_queries(Q)
+        np.testing.assert_allclose(R, dct_rotate(Q, signs), rtol=0, atol=2e-6)
+        port = port_cls(p)
+        ix.set_nprobe(6)
+        port.set_nprobe(6)
+        ids, ds, cnt = ix.search_batch(R, 10, transformed=True)
+        for i in range(len(R)):
+            pi, pd = port.search(R[i], 10, transformed=True)
+            assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd, ctx=f"dct {itype} q{i}")
+        ids2, _, cnt2 = ix.search_batch(Q, 10)
+        hits = sum(len(set(ids2[i, :cnt2[i]].tolist()) & set(port.search(Q[i], 10)[0].tolist()))
+                   for i in range(len(Q)))
+        assert hits >= 0.95 * 10 * len(Q)
+        port.close()
+        out = os.path.join(td, "saved.pdx")
+        ix.save(out)
+        assert open(out, "rb").read() == open(p, "rb").read()
+
+
 def test_save_roundtrip_bytes():
     for name in CASES:
         path, *_ = load_golden(name)

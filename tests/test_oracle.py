@@ -119,3 +119,18 @@ def test_port_recall_against_bruteforce(built_oracle):
         ids, ds, cnt = port.search_batch(Q, 10, n_threads=2)
         r = np.mean([recall(ids[i], gt[i], 10) for i in range(len(Q))])
         assert r >= 0.97  # exhaustive with ADSampling pruning
+
+
+def test_port_dct_rotation(built_oracle, tmp_path):
+    """FFTW-built files (1 x d sign vector): the port's rotation is the orthonormal DCT-II of
+    the sign-flipped query (adsampling.hpp:192-246)."""
+    from oracle.oracle import Port
+    from tests.helpers import dct_index, dct_rotate
+    f, Q, signs = dct_index("pdx_f32", 64, 3000, 12, seed=4)
+    p = str(tmp_path / "dct.pdx")
+    f.save(p)
+    port = Port(p)
+    ref = dct_rotate(Q[:8], signs)
+    for i in range(8):
+        np.testing.assert_allclose(port.prepare_query(Q[i]), ref[i], rtol=0, atol=2e-6)
+    port.close()
