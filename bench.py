@@ -123,6 +123,23 @@ def recall_at(ids, counts, gt, k):
     return hits / (k * len(gt))
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(x: float, device) -> float:
+    """The slowest rank's figure (1 process: x itself)."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_qps(queries_per_rank: int, steps: int, world: int, max_ms: float) -> float:
+    """All ranks' queries over the slowest rank's time (replicas: weak scaling)."""
+    return world * queries_per_rank * steps / (max_ms / 1e3)
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     def __init__(self, gpu_index: int):
@@ -348,12 +365,8 @@ def main():
     barrier()
     clocks = sampler.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * nq * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(sum(step_ms), device)
+    value = whole_job_qps(nq, args.steps, world, total_ms)
 
     # ---- roofline of the search kernel alone (prepared queries, same batch)
     prepared = torch.from_numpy(ix.prepare_queries(Qh)).to(device)
@@ -434,12 +447,8 @@ def main():
         t0 = time.perf_counter()
         e2e_step()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = statistics.mean(e2e_times)
-    e2e_value = nq / e2e_s
-    if world > 1:
-        t = torch.tensor([e2e_s], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * nq / float(t.item())
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), device)
+    e2e_value = whole_job_qps(nq, 1, world, e2e_s * 1e3)
 
     # ---- CPU baseline: the reference's own search on this host, bounded sample
     cpu = None
