@@ -61,6 +61,21 @@ int pdxg_load(const char* path, int device, pdxg_index** out);
 /* Same as pdxg_load, from an in-memory copy of the file bytes. */
 int pdxg_load_buffer(const void* data, uint64_t size, int device, pdxg_index** out);
 
+/* Replaces IPDXIndex::BuildIndex (index.hpp:174, 329-403 for PDXIndex, 640-758 for PDXTreeIndex;
+ * PDXIndexConfig index.hpp:27-40) and the pybind PDXIndex.build_index (python/lib.cpp:35): builds
+ * the index on `device` from `n` row-major float rows of `d` dims and loads it. `rotation` is the
+ * d x d row-major matrix applied to every (normalized, if `normalize`) row; index_type is one of
+ * PDXG_TYPE_*. num_clusters = 0 takes ComputeNumberOfClusters (common.hpp:191-199);
+ * num_meso_clusters = 0 takes sqrt(num_clusters) (trees only). k-means runs `kmeans_iters` Lloyd
+ * updates with BF16 tensor-core assignment (spherical for normalized data); the clustering is this
+ * engine's own, so cluster contents differ from the reference's (its SuperKMeans), while the file
+ * layout, the SQ8 parameters, the rotation and everything a search reads follow the reference.
+ * The same inputs and seed give the same index bytes. PDXG_ERR_UNSUPPORTED when d is not a
+ * multiple of 8 or the tensor-core GEMM is not available. */
+int pdxg_build(const float* data, uint64_t n, uint32_t d, uint32_t index_type, uint32_t num_clusters,
+               uint32_t num_meso_clusters, int normalize, const float* rotation, uint64_t seed,
+               uint32_t kmeans_iters, int device, pdxg_index** out);
+
 /* Releases the index and its GPU memory. NULL is ignored. */
 void pdxg_free(pdxg_index* index);
 

@@ -50,6 +50,8 @@ def library() -> C.CDLL:
         fn("pdxg_load", C.c_int, C.c_char_p, C.c_int, C.POINTER(vp))
         fn("pdxg_load_buffer", C.c_int, C.c_char_p, C.c_uint64, C.c_int, C.POINTER(vp))
         fn("pdxg_free", None, vp)
+        fn("pdxg_build", C.c_int, _f32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+           C.c_int, _f32p, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(vp))
         fn("pdxg_set_nprobe", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_pruning_aggressiveness", C.c_int, vp, C.c_float)
         fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
@@ -141,6 +143,29 @@ def _load_handle(path: Optional[str] = None, data: Optional[bytes] = None, devic
     return Handle(out.value)
 
 
+PDXG_ERR_UNSUPPORTED = 5
+
+
+def build_handle(data: np.ndarray, index_type: str, rotation: np.ndarray, num_clusters: int = 0,
+                 num_meso_clusters: int = 0, normalize: bool = False, seed: int = 42,
+                 kmeans_iters: int = 10, device: int = 0) -> Optional[Handle]:
+    """Builds an index on the GPU (pdxg_build). None when the engine cannot build this shape
+    (d not a multiple of 8); raises on every other error."""
+    lib = library()
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    rot = np.ascontiguousarray(rotation, dtype=np.float32)
+    n, d = data.shape
+    if rot.shape != (d, d):
+        raise ValueError(f"rotation must be {d} x {d}")
+    out = C.c_void_p()
+    rc = lib.pdxg_build(data, n, d, INDEX_TYPES[index_type], num_clusters, num_meso_clusters,
+                        1 if normalize else 0, rot, seed, kmeans_iters, device, C.byref(out))
+    if rc == PDXG_ERR_UNSUPPORTED:
+        return None
+    _check(rc)
+    return Handle(out.value)
+
+
 _METRICS = {0: "l2sq", 1: "cosine", 2: "ip"}
 
 
@@ -204,17 +229,17 @@ class PDXIndex:
             raise RuntimeError("data must be a 2D numpy array (n_embeddings x dimensions)")
         if data.shape[1] != self._d:
             raise ValueError(f"data has {data.shape[1]} dimensions, index expects {self._d}")
-        dev = None
-        try:
-            import torch
-            if torch.cuda.is_available():
-                dev = f"cuda:{self._device}"
-        except Exception:
-            dev = None
-        f = _build_index(data, self._type, num_clusters=self._num_clusters,
-                         num_meso_clusters=self._num_meso, normalize=self._normalize,
-                         seed=self._seed, kmeans_iters=self._kmeans_iters, device=dev)
-        self._h = _load_handle(data=f.to_bytes(), device=self._device)
+        from .builder import random_rotation
+        rotation = random_rotation(self._d, self._seed)
+        h = build_handle(data, self._type, rotation, self._num_clusters, self._num_meso, self._normalize,
+                         self._seed, self._kmeans_iters, self._device)
+        if h is None:  # d not a multiple of 8: k-means on torch's GPU GEMMs, same file layout
+            f = _build_index(data, self._type, num_clusters=self._num_clusters,
+                             num_meso_clusters=self._num_meso, normalize=self._normalize,
+                             seed=self._seed, kmeans_iters=self._kmeans_iters, rotation=rotation,
+                             device=f"cuda:{self._device}")
+            h = _load_handle(data=f.to_bytes(), device=self._device)
+        self._h = h
         _check(library().pdxg_set_nprobe(self._h.ptr, self._nprobe))
 
     def _handle(self) -> Handle:

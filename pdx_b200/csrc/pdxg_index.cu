@@ -1336,6 +1336,7 @@ uint32_t pdxg_index_dims(const pdxg_index* ix) { return ix->d; }
 std::mutex& pdxg_index_mutex(pdxg_index* ix) { return ix->mu; }
 cudaStream_t pdxg_index_stream(pdxg_index* ix) { return ix->stream; }
 int pdxg_set_error(int code, const char* msg) { return fail(code, msg); }
+void pdxg_split_dims(uint32_t d, uint32_t& h, uint32_t& v) { dimension_split(d, h, v); }
 
 namespace {
 
