@@ -123,8 +123,37 @@ int pdxg_filtered_search_batch(pdxg_index* index, const float* queries, uint32_t
                                const uint64_t* row_ids, const uint64_t* offsets, uint32_t flags,
                                uint32_t* ids, float* distances, uint32_t* counts);
 
-/* Replaces IPDXIndex::Save (index.hpp:173, 213-239, 483-514): writes the reference's format. */
+/* Replaces IPDXIndex::Save (index.hpp:173, 213-239, 483-514): writes the reference's format.
+ * After Append / Delete it first compacts every cluster, as the reference's tree Save does,
+ * which moves slots for later searches too. */
 int pdxg_save(pdxg_index* index, const char* path);
+
+/* Replaces PDXTreeIndex::Append (index.hpp:580-616) and PDXIndex.append (python/lib.cpp:51,
+ * lib.hpp:166-172): row_id must be the next row id (the row count so far); the embedding (d
+ * floats, host memory) is normalized when the index was built with normalize (an index loaded
+ * from a file keeps LoadPDXIndex's default config, which does not normalize: see
+ * pdxg_set_append_normalization) and rotated, then placed in the L1 cluster the top-level search
+ * finds (k = 1 over max(1, n_L0 / 8) meso clusters), in a tombstoned slot if the cluster has one
+ * (quantized with the index's SQ8 parameters for U8). PDXG_QUERY_TRANSFORMED in flags: the
+ * embedding is already normalized and rotated. Flat indexes answer PDXG_ERR_UNSUPPORTED
+ * ("Append is not implemented in PDXIndex", index.hpp:405-407). Not concurrent with searches. */
+int pdxg_append(pdxg_index* index, uint64_t row_id, const float* embedding, uint32_t flags);
+
+/* Replaces PDXTreeIndex::Delete (index.hpp:619-638) and PDXIndex.delete (python/lib.cpp:52):
+ * tombstones the row's slot. PDXG_ERR_INVALID_ARGUMENT for a row never appended or already
+ * deleted. After Append and Delete the cluster health check of index.hpp:1241-1255 runs: a full
+ * cluster with tombstones is compacted exactly as the reference does; where the reference would
+ * split a full cluster or merge a small one (SuperKMeans, not in the reference tree) this engine
+ * grows the cluster's capacity to max(1.3 x used, 256) slots, or keeps the cluster. */
+int pdxg_delete(pdxg_index* index, uint64_t row_id);
+
+/* PDXIndexConfig::normalize for Append (index.hpp:590-591): 1 for an index the caller built with
+ * normalize (pdxg_build sets it), 0 after pdxg_load (the reference's LoadPDXIndex default). */
+int pdxg_set_append_normalization(pdxg_index* index, int normalize);
+
+/* Maintenance counters: appends, deletes, compactions, capacity growths in place of splits,
+ * merges not performed, tombstoned slots now. */
+int pdxg_maintenance_stats(const pdxg_index* index, uint64_t out[6]);
 
 /* Getters: IPDXIndex::GetNumDimensions / GetNumClusters / GetClusterSize / GetClusterRowIds /
  * GetInMemorySizeInBytes (index.hpp:175-179) and the pybind getters (lib.hpp:148-164). */

@@ -198,6 +198,11 @@ class Reference(_Base):
                                  C.c_uint64, C.c_int, _u32p, _f32p)
         self._batch = self._fn("search_batch", C.c_int, vp, _f32p, C.c_uint32, C.c_uint32, C.c_int,
                                C.c_int, _u32p, _f32p, _u32p)
+        self._append = self._fn("append", C.c_int, vp, C.c_uint64, _f32p, C.c_int)
+        self._delete = self._fn("delete", C.c_int, vp, C.c_uint64)
+        self._set_append_norm = self._fn("set_append_normalization", None, vp, C.c_int)
+        self._compact_all = self._fn("compact_all", None, vp)
+        self._mstats = self._fn("maintenance_stats", None, vp, _u64p)
         self.h = self._load(path.encode())
         if not self.h:
             raise RuntimeError(self._err().decode())
@@ -226,6 +231,35 @@ class Reference(_Base):
         out = np.zeros(self._csize(self.h, c), np.uint32)
         self._cids(self.h, c, out)
         return out
+
+    # -- maintenance: PDXTreeIndex::Append / Delete on the reference's clusters ------------------
+    def _raise(self, rc: int):
+        msg = self._err().decode()
+        raise (ValueError if rc == 1 else RuntimeError)(msg)
+
+    def append(self, row_id: int, embedding, transformed: bool = False):
+        e = np.ascontiguousarray(embedding, dtype=np.float32)
+        rc = self._append(self.h, row_id, e, int(transformed))
+        if rc:
+            self._raise(rc)
+
+    def delete(self, row_id: int):
+        rc = self._delete(self.h, row_id)
+        if rc:
+            self._raise(rc)
+
+    def set_append_normalization(self, on: bool):
+        self._set_append_norm(self.h, int(on))
+
+    def compact_all(self):
+        """The compaction PDXTreeIndex::Save applies before writing (index.hpp:484-494)."""
+        self._compact_all(self.h)
+
+    def maintenance_stats(self) -> dict:
+        out = np.zeros(5, np.uint64)
+        self._mstats(self.h, out)
+        keys = ("appends", "deletes", "compactions", "capacity_growths", "merges_not_performed")
+        return {k: int(v) for k, v in zip(keys, out)}
 
     def rotate(self, X):
         X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float32)

@@ -11,6 +11,10 @@
 //   - PDXIndex / PDXTreeIndex ::Restore               (index.hpp:242-267, 516-543)
 //   - PDXTreeIndex::Search (top-level search + order) (index.hpp:545-566)
 //   - CreatePredicateEvaluator + BuildRowIdClusterMapping (index.hpp:421-446, 818-845)
+//   - PDXTreeIndex::Append / Delete / CheckClusterHealth and Save's compaction
+//     (index.hpp:580-638, 1241-1255, 484-494) on the reference's Cluster (cluster.hpp); the
+//     split and merge branches run SuperKMeans, so they are replaced by the substitutes the
+//     engine uses (capacity growth to max(uint32(1.3 used), 256); no merge)
 // Everything below those calls (IVF::Load, ADSamplingPruner, PDXearch::Search/FilteredSearch,
 // distance computers) is the reference's unmodified code.
 #include <cstddef>
@@ -30,6 +34,7 @@ extern "C" void sgemm_(const char* transa, const char* transb, const int* m, con
 #include "pdx/utils.hpp"
 
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <omp.h>
 #include <stdexcept>
@@ -53,6 +58,19 @@ struct RefIndexBase {
                                 bool transformed, std::vector<PDX::KNNCandidate>& out) = 0;
     virtual void SearchWithOrder(const float* q, uint32_t k, const uint32_t* order, size_t n_order,
                                  bool transformed, std::vector<PDX::KNNCandidate>& out) = 0;
+    // GetClusterRowIds (index.hpp:772-782): the used slots that are not tombstoned
+    virtual void LiveRowIds(uint32_t c, uint32_t* out) const {
+        std::memcpy(out, ClusterIds(c), sizeof(uint32_t) * ClusterSize(c));
+    }
+    virtual void Append(uint64_t, const float*, bool) {
+        throw std::runtime_error("Append is not implemented in PDXIndex. Use PDXTreeIndex instead.");
+    }
+    virtual void Delete(uint64_t) {
+        throw std::runtime_error("Delete is not implemented in PDXIndex. Use PDXTreeIndex instead.");
+    }
+    virtual void CompactAll() {}
+    bool append_normalize = false;  // PDXIndexConfig::normalize (false after LoadPDXIndex)
+    uint64_t maint_stats[5] = {0, 0, 0, 0, 0};  // appends, deletes, compactions, growths, merges
 };
 
 template <class IndexT, PDX::Quantization Q>
@@ -63,6 +81,7 @@ PDX::PredicateEvaluator MakeEvaluator(const IndexT& index,
     for (size_t i = 0; i < n; ++i) {
         if (row_ids[i] >= mapping.size()) continue;
         const auto& [cluster_id, pos] = mapping[row_ids[i]];
+        if (cluster_id == std::numeric_limits<uint32_t>::max()) continue;  // DELETED_MARKER
         ev.n_passing_tuples[cluster_id]++;
         ev.selection_vector[index.cluster_offsets[cluster_id] + pos] = 1;
     }
@@ -163,6 +182,110 @@ struct RefTree : RefIndexBase {
         s.SetClusterAccessOrder(std::vector<uint32_t>(order, order + n_order));
         out = s.Search(q, k, transformed);
     }
+    void LiveRowIds(uint32_t c, uint32_t* out) const override {
+        const auto& cl = index.clusters[c];
+        uint32_t j = 0;
+        for (uint32_t i = 0; i < cl.used_capacity; i++)
+            if (!cl.HasTombstone(i)) out[j++] = cl.indices[i];
+    }
+
+    static constexpr uint32_t kDeleted = std::numeric_limits<uint32_t>::max();  // index.hpp:462
+
+    // PDXTreeIndex::Append (index.hpp:580-616)
+    void Append(uint64_t row_id, const float* embedding, bool transformed) override {
+        if (row_id != mapping.size())
+            throw std::invalid_argument("Append: row_id " + std::to_string(row_id) +
+                                        " is not sequential (expected " + std::to_string(mapping.size()) + ")");
+        const uint32_t d = index.num_dimensions;
+        std::unique_ptr<float[]> pre(new float[d]);
+        if (transformed) {
+            std::memcpy(pre.get(), embedding, sizeof(float) * d);
+        } else {  // NormalizeAndRotate (index.hpp:75-97)
+            const float* in = embedding;
+            std::unique_ptr<float[]> normalized;
+            if (append_normalize) {
+                normalized.reset(new float[d]);
+                PDX::Quantizer qz(d);
+                qz.NormalizeQuery(embedding, normalized.get());
+                in = normalized.get();
+            }
+            pruner->PreprocessEmbeddings(in, pre.get(), 1);
+        }
+        PDX::PDXearch<PDX::F32> top(index.l0, *pruner);
+        top.SetNProbe(std::max(1u, index.l0.num_clusters / 8));
+        auto cand = top.Search(pre.get(), 1, true);
+        const uint32_t c = cand[0].index;
+        auto& cluster = index.clusters[c];
+        uint32_t pos;
+        if constexpr (Q == PDX::U8) {  // QuantizeAndAppend (index.hpp:885-896)
+            std::unique_ptr<uint8_t[]> qv(new uint8_t[d]);
+            PDX::ScalarQuantizer<Q> quantizer(d);
+            quantizer.QuantizeEmbedding(pre.get(), index.quantization_base, index.quantization_scale, qv.get());
+            pos = cluster.AppendEmbedding(static_cast<uint32_t>(row_id), qv.get());
+        } else {
+            pos = cluster.AppendEmbedding(static_cast<uint32_t>(row_id), pre.get());
+        }
+        mapping.emplace_back(c, pos);
+        index.total_num_embeddings++;
+        maint_stats[0]++;
+        CheckHealth(c);
+    }
+
+    // PDXTreeIndex::Delete (index.hpp:619-638)
+    void Delete(uint64_t row_id) override {
+        if (row_id >= mapping.size())
+            throw std::invalid_argument("Delete: row_id " + std::to_string(row_id) + " is not in the index");
+        const auto [c, pos] = mapping[row_id];
+        if (c == kDeleted)
+            throw std::invalid_argument("Delete: row_id " + std::to_string(row_id) + " was already deleted");
+        index.clusters[c].DeleteEmbedding(pos);
+        mapping[row_id] = {kDeleted, kDeleted};
+        index.total_num_embeddings--;
+        maint_stats[1]++;
+        CheckHealth(c);
+    }
+
+    // CheckClusterHealth (index.hpp:1241-1255) with the split / merge substitutes
+    void CheckHealth(uint32_t c) {
+        auto& cluster = index.clusters[c];
+        if (cluster.used_capacity == cluster.max_capacity) {
+            if (cluster.num_embeddings < cluster.used_capacity) {
+                for (const auto& [rid, idx] : cluster.CompactCluster()) mapping[rid] = {c, idx};
+                maint_stats[2]++;
+            } else {
+                Grow(c);
+            }
+        } else if (cluster.num_embeddings <= cluster.min_capacity) {
+            maint_stats[4]++;
+        }
+    }
+
+    // In place of SplitCluster: the same rows, in the same slots, in a buffer of
+    // max(uint32(1.3 used), 256) slots.
+    void Grow(uint32_t c) {
+        auto& old = index.clusters[c];
+        const uint32_t d = index.num_dimensions;
+        uint32_t cap = std::max<uint32_t>(static_cast<uint32_t>(static_cast<float>(old.used_capacity) * 1.3f), 256u);
+        if (cap <= old.used_capacity) cap = old.used_capacity + 1;
+        auto rows = old.GetHorizontalEmbeddingsFromPDXBuffer();
+        PDX::Cluster<Q> grown(0u, cap, d);
+        for (uint32_t i = 0; i < old.num_embeddings; i++)
+            grown.AppendEmbedding(old.indices[i], rows.get() + static_cast<size_t>(i) * d);
+        grown.min_capacity = old.min_capacity;
+        grown.id = old.id;
+        grown.mesocluster_id = old.mesocluster_id;
+        index.clusters[c] = std::move(grown);
+        index.ComputeClusterOffsets();
+        maint_stats[3]++;
+    }
+
+    // The compaction of PDXTreeIndex::Save (index.hpp:484-494)
+    void CompactAll() override {
+        for (uint32_t c = 0; c < index.num_clusters; c++)
+            for (const auto& [rid, idx] : index.clusters[c].CompactCluster()) mapping[rid] = {c, idx};
+        for (uint32_t c = 0; c < index.l0.num_clusters; c++) index.l0.clusters[c].CompactCluster();
+    }
+
     void RebuildL1Centroids() {
         const uint32_t d = index.num_dimensions;
         std::vector<float> cents(static_cast<size_t>(index.num_clusters) * d, 0.0f);
@@ -270,9 +393,46 @@ uint32_t pdxref_cluster_size(void* h, uint32_t c) {
     return static_cast<RefIndexBase*>(h)->ClusterSize(c);
 }
 void pdxref_cluster_row_ids(void* h, uint32_t c, uint32_t* out) {
-    auto* r = static_cast<RefIndexBase*>(h);
-    std::memcpy(out, r->ClusterIds(c), sizeof(uint32_t) * r->ClusterSize(c));
+    static_cast<RefIndexBase*>(h)->LiveRowIds(c, out);
 }
+
+// 0, 1 (std::invalid_argument) or 2 (other error); the message in pdxref_last_error.
+int pdxref_append(void* h, uint64_t row_id, const float* embedding, int transformed) {
+    try {
+        static_cast<RefIndexBase*>(h)->Append(row_id, embedding, transformed != 0);
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return 1;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 2;
+    }
+}
+
+int pdxref_delete(void* h, uint64_t row_id) {
+    try {
+        static_cast<RefIndexBase*>(h)->Delete(row_id);
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return 1;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 2;
+    }
+}
+
+void pdxref_set_append_normalization(void* h, int on) {
+    static_cast<RefIndexBase*>(h)->append_normalize = on != 0;
+}
+
+void pdxref_compact_all(void* h) { static_cast<RefIndexBase*>(h)->CompactAll(); }
+
+void pdxref_maintenance_stats(void* h, uint64_t* out) {
+    std::memcpy(out, static_cast<RefIndexBase*>(h)->maint_stats, sizeof(uint64_t) * 5);
+}
+
 
 void pdxref_set_nprobe(void* h, uint32_t nprobe) { static_cast<RefIndexBase*>(h)->nprobe = nprobe; }
 

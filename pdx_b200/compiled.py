@@ -93,6 +93,10 @@ def library() -> C.CDLL:
         fn("pdxg_search_requests", C.c_int, vp, vp, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, vp, vp, vp)
         fn("pdxg_filter_register", C.c_int, vp, vp, C.c_uint64, C.POINTER(C.c_int32))
         fn("pdxg_filter_release", C.c_int, vp, C.c_int32)
+        fn("pdxg_append", C.c_int, vp, C.c_uint64, _f32p, C.c_uint32)
+        fn("pdxg_delete", C.c_int, vp, C.c_uint64)
+        fn("pdxg_set_append_normalization", C.c_int, vp, C.c_int)
+        fn("pdxg_maintenance_stats", C.c_int, vp, _u64p)
         _lib = lib
     return _lib
 
@@ -239,6 +243,7 @@ class PDXIndex:
                              seed=self._seed, kmeans_iters=self._kmeans_iters, rotation=rotation,
                              device=f"cuda:{self._device}")
             h = _load_handle(data=f.to_bytes(), device=self._device)
+            _check(library().pdxg_set_append_normalization(h.ptr, 1 if self._normalize else 0))
         self._h = h
         _check(library().pdxg_set_nprobe(self._h.ptr, self._nprobe))
 
@@ -464,15 +469,34 @@ class PDXIndex:
         return self._handle()
 
     # -- maintenance (tree indexes in the reference) -----------------------------------
-    def append(self, row_id: int, embedding: np.ndarray) -> None:
+    def append(self, row_id: int, embedding: np.ndarray, transformed: bool = False) -> None:
+        """PDXTreeIndex::Append (index.hpp:580-616); transformed: the embedding is already
+        normalized and rotated (extension)."""
         if self._type in ("pdx_f32", "pdx_u8"):
             raise RuntimeError("Append is not implemented in PDXIndex. Use PDXTreeIndex instead.")
-        raise RuntimeError("Append is not supported by the GPU engine yet")
+        e = np.ascontiguousarray(embedding, dtype=np.float32)
+        if e.ndim != 1:
+            raise RuntimeError("embedding must be a 1D numpy array")
+        if e.shape[0] != self._d:
+            raise ValueError(f"embedding has {e.shape[0]} dimensions, index expects {self._d}")
+        if row_id < 0:
+            raise ValueError(f"Append: row_id {row_id} is not sequential")
+        _check(library().pdxg_append(self._handle().ptr, int(row_id), e,
+                                     PDXG_QUERY_TRANSFORMED if transformed else 0))
 
     def delete(self, row_id: int) -> None:
+        """PDXTreeIndex::Delete (index.hpp:619-638)."""
         if self._type in ("pdx_f32", "pdx_u8"):
             raise RuntimeError("Delete is not implemented in PDXIndex. Use PDXTreeIndex instead.")
-        raise RuntimeError("Delete is not supported by the GPU engine yet")
+        if row_id < 0:
+            raise ValueError(f"Delete: row_id {row_id} is not in the index")
+        _check(library().pdxg_delete(self._handle().ptr, int(row_id)))
+
+    def maintenance_stats(self) -> dict:
+        out = np.zeros(6, np.uint64)
+        _check(library().pdxg_maintenance_stats(self._handle().ptr, out))
+        keys = ("appends", "deletes", "compactions", "capacity_growths", "merges_not_performed", "tombstones")
+        return {k: int(v) for k, v in zip(keys, out)}
 
 
 # pdxg_request (include/pdx_b200.h)

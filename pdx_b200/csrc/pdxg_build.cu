@@ -487,5 +487,7 @@ extern "C" int pdxg_build(const float* data, uint64_t n, uint32_t d, uint32_t in
         put_bytes(file, &base, 4);
         put_bytes(file, &scale, 4);
     }
-    return pdxg_load_buffer(file.data(), file.size(), device, out);
+    int rc = pdxg_load_buffer(file.data(), file.size(), device, out);
+    if (rc == PDXG_OK) pdxg_set_append_normalization(*out, normalize);
+    return rc;
 }

@@ -25,10 +25,10 @@ struct DevCluster {
     uint64_t vert_off;  // vertical block
     uint64_t hor_off;   // horizontal blocks
     uint64_t ids_off;   // row ids
-    uint32_t n;         // vectors in the cluster (used capacity)
+    uint32_t n;         // vectors in the cluster (used capacity, tombstoned slots included)
     uint32_t n_pad;     // row stride in vectors (multiple of 32)
     uint32_t sel_word;  // first 32-bit word of this cluster in a filter selection bitmap
-    uint32_t pad_;
+    uint32_t live;      // vectors not tombstoned (num_embeddings); n when there are none
 };
 
 struct DevLevel {
@@ -45,6 +45,8 @@ struct DevLevel {
     float scale_sq;              // U8: quantization_scale^2
     float inv_scale_sq;          // U8: 1 / quantization_scale^2
     float base, scale;           // U8 quantization parameters
+    const uint32_t* tomb;        // tombstoned slots, one bit per slot in the selection-bitmap
+                                 // layout (sel_word); null when the level has none
 };
 
 // One batched search launch.

@@ -11,10 +11,12 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <atomic>
 #include <functional>
 #include <mutex>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/pdx_b200.h"
@@ -188,7 +190,7 @@ uint64_t plan_level(HostLevel& lv, uint64_t off) {
         m.n = n;
         m.n_pad = n_pad;
         m.sel_word = sel;
-        m.pad_ = 0;
+        m.live = n;
         sel += n_pad / 32;
         off = align_up(off, 256);
         m.vert_off = off;
@@ -324,6 +326,28 @@ void free_workspace(Workspace& w) {
     w = Workspace();
 }
 
+// Mutable state of a tree index once Append / Delete have been used (PDXTreeIndex,
+// index.hpp:580-638, and Cluster, cluster.hpp:86-154, 260-294).
+struct MaintCluster {
+    uint32_t num_embeddings = 0, used = 0, max_cap = 0, min_cap = 0;
+    // the reference's container (cluster.hpp:20): PopTombstone takes begin(), so the same
+    // sequence of inserts and erases reuses and compacts the same slots
+    std::unordered_set<uint32_t> tombstones;
+    std::vector<uint32_t> indices;  // row id of every used slot
+};
+
+struct Maint {
+    std::vector<MaintCluster> cl;
+    uint64_t arena_cap = 0;       // bytes allocated for the arena (arena_bytes are in use)
+    uint32_t* d_tomb = nullptr;   // tombstone bitmap in the selection-bitmap layout
+    uint64_t tomb_cap = 0;        // words allocated
+    std::vector<uint32_t> tomb;   // host copy (l1.sel_words words)
+    uint64_t n_tomb = 0;          // tombstoned slots over all clusters
+    uint64_t live = 0;            // total_num_embeddings
+    uint64_t rid_cap = 0;         // entries allocated for the device row maps
+    uint64_t appends = 0, deletes = 0, compactions = 0, grown = 0, merges_deferred = 0;
+};
+
 }  // namespace
 
 struct pdxg_index {
@@ -389,8 +413,19 @@ struct pdxg_index {
     uint32_t* d_reg_pass = nullptr;  // [reg_cap x l1 clusters]
     uint32_t reg_cap = 0;
     std::vector<uint8_t> reg_used;
+    std::vector<std::vector<uint64_t>> reg_rows;  // row ids of each registered filter
+    bool reg_dirty = false;  // slots moved since the bitmaps were built (Append / Delete)
     std::mutex reg_mu;
+    // Append / Delete (tree indexes): created on first use
+    std::unique_ptr<Maint> maint;
+    uint64_t l0_start = 0;          // first arena byte of the meso level
+    bool append_normalize = false;  // PDXIndexConfig::normalize: set by a build, false after a
+                                    // load (LoadPDXIndex uses the default config)
 };
+
+// Append / Delete support (maintenance section at the end of this file).
+int maint_prepare_save(pdxg_index* ix);
+int refresh_registered_filters(pdxg_index* ix);
 
 namespace {
 
@@ -419,8 +454,9 @@ int upload_ratios(pdxg_index* ix) {
 }
 
 DevLevel make_level(const HostLevel& lv, const DevCluster* dcl, const float* cent, float base,
-                    float scale) {
+                    float scale, const uint32_t* tomb = nullptr) {
     DevLevel L{};
+    L.tomb = tomb;
     L.clusters = dcl;
     L.centroids = cent;
     L.nclusters = (uint32_t)lv.fc.size();
@@ -461,6 +497,7 @@ void free_index(pdxg_index* ix) {
     cudaFree(ix->d_rid_pos);
     cudaFree(ix->d_reg_sel);
     cudaFree(ix->d_reg_pass);
+    if (ix->maint) cudaFree(ix->maint->d_tomb);
     for (cudaEvent_t e : ix->tev)
         if (e) cudaEventDestroy(e);
     free_workspace(ix->ws);
@@ -601,6 +638,7 @@ int load_from_bytes(const uint8_t* buf, uint64_t size, int device, pdxg_index** 
     if (ix->tree) {
         for (DevCluster& m : ix->l0.meta) (void)m;
         const uint64_t start0 = off;
+        ix->l0_start = start0;
         off = plan_level(ix->l0, start0);
     }
     ix->arena_bytes = off;
@@ -705,7 +743,8 @@ int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool 
                 bool probe_ahead = false) {
     SearchParams& p = L.p;
     p.arena = ix->arena;
-    p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale);
+    p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale,
+                      (ix->maint && ix->maint->n_tomb) ? ix->maint->d_tomb : nullptr);
     p.is_tree = ix->tree ? 1 : 0;
     if (ix->tree) p.l0 = make_level(ix->l0, ix->d_cl0, ix->d_cent0, 0.0f, 1.0f);
     p.ratios = ix->d_ratios;
@@ -799,9 +838,13 @@ int ensure_ws(pdxg_index* ix, Workspace& w, uint32_t nq, uint32_t k) {
 
 // NormalizeQuery + rotation of nq device queries into `out` (ADSamplingPruner::PreprocessQuery,
 // adsampling.hpp:100-113): TF32x3 tensor-core GEMM when available, else the FP32 SIMT GEMM.
-int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float* out, cudaStream_t st) {
+// normalize: -1 follows the index's is_normalized flag (queries), 0 / 1 force it (appended rows
+// follow PDXIndexConfig::normalize).
+int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float* out, cudaStream_t st,
+                int normalize = -1) {
     if (nq == 0) return PDXG_OK;
     const uint32_t d = ix->d;
+    const bool norm = normalize < 0 ? ix->normalized : normalize != 0;
     if (ix->rot_tc && ix->rot_mode == 0) {
         int rc;
         if ((rc = dev_grow(w.d_qhi, w.qhi_cap, (uint64_t)nq * d))) return rc;
@@ -810,7 +853,7 @@ int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float
             PDXG_CUDA(cudaMalloc(&w.d_gemm_err, sizeof(int)));
             PDXG_CUDA(cudaMemsetAsync(w.d_gemm_err, 0, sizeof(int), st));
         }
-        PDXG_CUDA(launch_split_rows(q, nq, d, ix->normalized, w.d_qhi, w.d_qlo, st));
+        PDXG_CUDA(launch_split_rows(q, nq, d, norm, w.d_qhi, w.d_qlo, st));
         GemmOperand a;
         if (make_gemm_operand(a, kGemmTF32x3, w.d_qhi, w.d_qlo, nq, d) != 0)
             return fail(PDXG_ERR_CUDA, "cannot encode the query tensor maps");
@@ -824,7 +867,7 @@ int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float
         PDXG_CUDA(launch_gemm(a, ix->rot_op, kEpiStore, g, st));
         return PDXG_OK;
     }
-    PDXG_CUDA(launch_prepare_queries(q, nq, d, ix->d_rot, ix->normalized, w.d_norms, out, st));
+    PDXG_CUDA(launch_prepare_queries(q, nq, d, ix->d_rot, norm, w.d_norms, out, st));
     return PDXG_OK;
 }
 
@@ -1867,19 +1910,30 @@ int pdxg_index_type(const pdxg_index* ix) { return ix ? ix->type : -1; }
 uint32_t pdxg_num_dimensions(const pdxg_index* ix) { return ix ? ix->d : 0; }
 uint32_t pdxg_num_clusters(const pdxg_index* ix) { return ix ? (uint32_t)ix->l1.fc.size() : 0; }
 uint32_t pdxg_nprobe(const pdxg_index* ix) { return ix ? ix->nprobe : 0; }
-uint64_t pdxg_num_embeddings(const pdxg_index* ix) { return ix ? ix->l1.total_vectors : 0; }
+uint64_t pdxg_num_embeddings(const pdxg_index* ix) {
+    if (!ix) return 0;
+    return ix->maint ? ix->maint->live : ix->l1.total_vectors;
+}
 
+// GetClusterSize / GetClusterRowIds (index.hpp:768-782): tombstoned slots are left out.
 uint32_t pdxg_cluster_size(const pdxg_index* ix, uint32_t cluster_id) {
     if (!ix || cluster_id >= ix->l1.n.size()) return 0;
-    return ix->l1.n[cluster_id];
+    return ix->maint ? ix->maint->cl[cluster_id].num_embeddings : ix->l1.n[cluster_id];
 }
 
 int pdxg_cluster_row_ids(const pdxg_index* ix, uint32_t cluster_id, uint32_t* out,
                          uint32_t capacity) {
     if (int rc = check_index(ix)) return rc;
     if (cluster_id >= ix->l1.n.size()) return fail(PDXG_ERR_INVALID_ARGUMENT, "cluster_id out of range");
-    const uint32_t n = ix->l1.n[cluster_id];
+    const uint32_t n = pdxg_cluster_size(ix, cluster_id);
     if (capacity < n || (!out && n)) return fail(PDXG_ERR_INVALID_ARGUMENT, "output buffer too small");
+    if (ix->maint) {
+        const MaintCluster& K = ix->maint->cl[cluster_id];
+        uint32_t j = 0;
+        for (uint32_t i = 0; i < K.used; ++i)
+            if (!K.tombstones.count(i)) out[j++] = K.indices[i];
+        return PDXG_OK;
+    }
     std::memcpy(out, ix->l1.ids.data() + ix->l1.ids_start[cluster_id], (size_t)n * 4);
     return PDXG_OK;
 }
@@ -1897,6 +1951,10 @@ int pdxg_save(pdxg_index* ix, const char* path) {
     if (!path) return fail(PDXG_ERR_INVALID_ARGUMENT, "path is NULL");
     std::lock_guard<std::mutex> lock(ix->mu);
     PDXG_CUDA(cudaSetDevice(ix->device));
+    if (ix->maint) {
+        std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
+        if (int rc = maint_prepare_save(ix)) return rc;
+    }
     std::vector<uint8_t> img(ix->arena_bytes);
     PDXG_CUDA(cudaMemcpy(img.data(), ix->arena, ix->arena_bytes, cudaMemcpyDeviceToHost));
     std::ofstream out(path, std::ios::binary);
@@ -2063,6 +2121,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
     if (nq == 0) return PDXG_OK;
     // the registry cannot grow (and move) between the checks below and the launch
     std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
+    if (int rc = refresh_registered_filters(ix)) return rc;
     // resolve every query's parameters as PDXearch / PDXTreeIndex::Search would
     const uint32_t n1 = (uint32_t)ix->l1.fc.size();
     const uint32_t n0 = (uint32_t)ix->l0.fc.size();
@@ -2194,6 +2253,7 @@ int pdxg_filter_register(pdxg_index* ix, const uint64_t* row_ids, uint64_t n, in
     if (n && !row_ids) return fail(PDXG_ERR_INVALID_ARGUMENT, "row_ids is NULL");
     std::lock_guard<std::mutex> lock(ix->reg_mu);
     PDXG_CUDA(cudaSetDevice(ix->device));
+    if (int rc = refresh_registered_filters(ix)) return rc;
     const uint32_t words = ix->l1.sel_words;
     const uint32_t n1 = (uint32_t)ix->l1.fc.size();
     uint32_t slot = 0;
@@ -2219,6 +2279,7 @@ int pdxg_filter_register(pdxg_index* ix, const uint64_t* row_ids, uint64_t n, in
         ix->d_reg_pass = pass;
         ix->reg_cap = cap;
         ix->reg_used.resize(cap, 0);
+        ix->reg_rows.resize(cap);
     }
     std::vector<uint32_t> sel(words, 0), pass(n1, 0);
     build_filter(ix, row_ids, n, sel.data(), pass.data());
@@ -2227,6 +2288,7 @@ int pdxg_filter_register(pdxg_index* ix, const uint64_t* row_ids, uint64_t n, in
     PDXG_CUDA(cudaMemcpy(ix->d_reg_pass + (size_t)slot * n1, pass.data(), (size_t)n1 * 4,
                          cudaMemcpyHostToDevice));
     ix->reg_used[slot] = 1;
+    if (ix->tree) ix->reg_rows[slot].assign(row_ids, row_ids + n);  // rebuilt after Append / Delete
     *filter_id = (int32_t)slot;
     return PDXG_OK;
 }
@@ -2237,6 +2299,572 @@ int pdxg_filter_release(pdxg_index* ix, int32_t filter_id) {
     if (filter_id < 0 || (uint32_t)filter_id >= ix->reg_cap || !ix->reg_used[filter_id])
         return fail(PDXG_ERR_INVALID_ARGUMENT, "unknown filter id " + std::to_string(filter_id));
     ix->reg_used[filter_id] = 0;
+    ix->reg_rows[filter_id].clear();
+    ix->reg_rows[filter_id].shrink_to_fit();
+    return PDXG_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================== maintenance
+// PDXTreeIndex::Append / Delete (index.hpp:580-638) on the device-resident index. The first call
+// re-lays the L1 clusters at their max_capacity strides (the buffer of Cluster, cluster.hpp:26-38),
+// so an append, a delete and a compaction touch single slots in place; the meso level is copied
+// unchanged. The host keeps each cluster's counters, tombstone set and row ids; the device gets the
+// slot data, the cluster records and a tombstone bitmap that the scan masks exactly where the
+// reference's searcher does (searcher.hpp:169-179 and its callers).
+// Split and merge maintenance (index.hpp:1000-1729) runs the reference's SuperKMeans, whose
+// sources are not part of the reference tree: where the reference would split a full cluster
+// (used == max_capacity, no tombstones) this engine grows the cluster's capacity to
+// max(uint32(1.3 used), 256) slots, and where it would merge a cluster (num_embeddings <=
+// min_capacity) it keeps the cluster. Both are counted (pdxg_maintenance_stats); results equal the
+// reference's up to the first such event.
+namespace {
+
+constexpr uint32_t kNoCluster = 0xFFFFFFFFu;  // DELETED_MARKER (index.hpp:462)
+
+uint32_t slot_stride(uint32_t cap) { return std::max<uint32_t>(32, (cap + 31) / 32 * 32); }
+
+uint64_t cluster_block_bytes(const HostLevel& lv, uint32_t np) {
+    const uint64_t esz = lv.u8 ? 1 : 4;
+    return align_up((uint64_t)lv.n_vwords * np * 4, 256) + align_up((uint64_t)lv.n_hblocks * np * kHDim * esz, 256) +
+           align_up((uint64_t)np * 4, 256);
+}
+
+// Cluster record m placed at arena offset off (256-byte aligned) with a stride of np slots.
+void place_cluster(const HostLevel& lv, DevCluster& m, uint64_t off, uint32_t np) {
+    const uint64_t esz = lv.u8 ? 1 : 4;
+    m.n_pad = np;
+    m.vert_off = off;
+    off = align_up(off + (uint64_t)lv.n_vwords * np * 4, 256);
+    m.hor_off = off;
+    off = align_up(off + (uint64_t)lv.n_hblocks * np * kHDim * esz, 256);
+    m.ids_off = off;
+}
+
+// The first n slots of cluster src (in src_arena) into cluster dst (in dst_arena).
+cudaError_t copy_cluster_slots(const HostLevel& lv, uint8_t* dst_arena, const DevCluster& dst,
+                               const uint8_t* src_arena, const DevCluster& src, uint32_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const size_t esz = lv.u8 ? 1 : 4;
+    cudaError_t e = cudaMemcpy2DAsync(dst_arena + dst.vert_off, (size_t)dst.n_pad * 4, src_arena + src.vert_off,
+                                      (size_t)src.n_pad * 4, (size_t)n * 4, lv.n_vwords, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && lv.n_hblocks)
+        e = cudaMemcpy2DAsync(dst_arena + dst.hor_off, (size_t)dst.n_pad * kHDim * esz, src_arena + src.hor_off,
+                              (size_t)src.n_pad * kHDim * esz, (size_t)n * kHDim * esz, lv.n_hblocks,
+                              cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dst_arena + dst.ids_off, src_arena + src.ids_off, (size_t)n * 4, cudaMemcpyDeviceToDevice,
+                            st);
+    return e;
+}
+
+// Slot `from` of a cluster copied over slot `to` (CopyEmbeddingInPDXLayout, cluster.hpp).
+cudaError_t move_slot(const HostLevel& lv, uint8_t* arena, const DevCluster& m, uint32_t from, uint32_t to,
+                      cudaStream_t st) {
+    const size_t esz = lv.u8 ? 1 : 4;
+    const size_t vp = (size_t)m.n_pad * 4, hr = (size_t)kHDim * esz, hp = (size_t)m.n_pad * hr;
+    cudaError_t e = cudaMemcpy2DAsync(arena + m.vert_off + (size_t)to * 4, vp, arena + m.vert_off + (size_t)from * 4, vp,
+                                      4, lv.n_vwords, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && lv.n_hblocks)
+        e = cudaMemcpy2DAsync(arena + m.hor_off + (size_t)to * hr, hp, arena + m.hor_off + (size_t)from * hr, hp, hr,
+                              lv.n_hblocks, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(arena + m.ids_off + (size_t)to * 4, arena + m.ids_off + (size_t)from * 4, 4,
+                            cudaMemcpyDeviceToDevice, st);
+    return e;
+}
+
+// One row into slot `slot`: vertical words (4 bytes each: an F32 dim, or 4 interleaved U8 dims),
+// the horizontal 64-dim blocks and the row id, from host memory.
+cudaError_t write_slot(const HostLevel& lv, uint8_t* arena, const DevCluster& m, uint32_t slot,
+                       const uint32_t* vwords, const uint8_t* hrow, const uint32_t* row_id, cudaStream_t st) {
+    const size_t esz = lv.u8 ? 1 : 4;
+    const size_t hr = (size_t)kHDim * esz;
+    cudaError_t e = cudaMemcpy2DAsync(arena + m.vert_off + (size_t)slot * 4, (size_t)m.n_pad * 4, vwords, 4, 4,
+                                      lv.n_vwords, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && lv.n_hblocks)
+        e = cudaMemcpy2DAsync(arena + m.hor_off + (size_t)slot * hr, (size_t)m.n_pad * hr, hrow, hr, hr, lv.n_hblocks,
+                              cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(arena + m.ids_off + (size_t)slot * 4, row_id, 4, cudaMemcpyHostToDevice, st);
+    return e;
+}
+
+int upload_cluster_record(pdxg_index* ix, uint32_t c, cudaStream_t st) {
+    PDXG_CUDA(cudaMemcpyAsync(ix->d_cl1 + c, &ix->l1.meta[c], sizeof(DevCluster), cudaMemcpyHostToDevice, st));
+    return PDXG_OK;
+}
+
+// Cluster c's record after its counters changed.
+int sync_cluster(pdxg_index* ix, uint32_t c, cudaStream_t st) {
+    const MaintCluster& K = ix->maint->cl[c];
+    DevCluster& m = ix->l1.meta[c];
+    m.n = K.used;
+    m.live = K.num_embeddings;
+    ix->l1.n[c] = K.used;
+    ix->l1.max_n = std::max(ix->l1.max_n, K.used);
+    return upload_cluster_record(ix, c, st);
+}
+
+int set_tombstone_bit(pdxg_index* ix, uint32_t c, uint32_t slot, bool on, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    const uint32_t w = ix->l1.meta[c].sel_word + (slot >> 5);
+    const uint32_t bit = 1u << (slot & 31);
+    M.tomb[w] = on ? (M.tomb[w] | bit) : (M.tomb[w] & ~bit);
+    M.n_tomb += on ? 1 : 0;
+    M.n_tomb -= on ? 0 : 1;
+    PDXG_CUDA(cudaMemcpyAsync(M.d_tomb + w, &M.tomb[w], 4, cudaMemcpyHostToDevice, st));
+    return PDXG_OK;
+}
+
+int upload_row_map(pdxg_index* ix, uint64_t r, cudaStream_t st) {
+    PDXG_CUDA(cudaMemcpyAsync(ix->d_rid_cluster + r, &ix->rid_cluster[r], 4, cudaMemcpyHostToDevice, st));
+    PDXG_CUDA(cudaMemcpyAsync(ix->d_rid_pos + r, &ix->rid_pos[r], 4, cudaMemcpyHostToDevice, st));
+    return PDXG_OK;
+}
+
+int grow_row_maps(pdxg_index* ix, uint64_t need, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    if (need <= M.rid_cap) return PDXG_OK;
+    const uint64_t cap = std::max<uint64_t>({need, M.rid_cap * 2, 1024});
+    uint32_t *c = nullptr, *p = nullptr;
+    if (cudaMalloc(&c, cap * 4) != cudaSuccess || cudaMalloc(&p, cap * 4) != cudaSuccess) {
+        cudaFree(c);
+        return fail(PDXG_ERR_CUDA, "cannot grow the row id map");
+    }
+    const uint64_t have = std::min<uint64_t>(ix->rid_cluster.size(), M.rid_cap);
+    if (have) {
+        PDXG_CUDA(cudaMemcpyAsync(c, ix->d_rid_cluster, have * 4, cudaMemcpyDeviceToDevice, st));
+        PDXG_CUDA(cudaMemcpyAsync(p, ix->d_rid_pos, have * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    cudaFree(ix->d_rid_cluster);
+    cudaFree(ix->d_rid_pos);
+    ix->d_rid_cluster = c;
+    ix->d_rid_pos = p;
+    M.rid_cap = cap;
+    return PDXG_OK;
+}
+
+// Selection-bitmap words of every L1 cluster from its stride, the tombstone bitmap in that
+// layout, and every record uploaded (after a cluster's stride changed).
+int relayout_bitmaps(pdxg_index* ix, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    HostLevel& lv = ix->l1;
+    uint32_t sel = 0;
+    for (DevCluster& m : lv.meta) {
+        m.sel_word = sel;
+        sel += m.n_pad / 32;
+    }
+    lv.sel_words = sel;
+    M.tomb.assign(sel, 0u);
+    for (size_t c = 0; c < M.cl.size(); ++c)
+        for (uint32_t t : M.cl[c].tombstones) M.tomb[lv.meta[c].sel_word + (t >> 5)] |= 1u << (t & 31);
+    if (sel > M.tomb_cap) {
+        cudaFree(M.d_tomb);
+        M.d_tomb = nullptr;
+        M.tomb_cap = 0;
+        PDXG_CUDA(cudaMalloc(&M.d_tomb, (size_t)sel * 4));
+        M.tomb_cap = sel;
+    }
+    PDXG_CUDA(cudaMemcpyAsync(M.d_tomb, M.tomb.data(), (size_t)sel * 4, cudaMemcpyHostToDevice, st));
+    PDXG_CUDA(cudaMemcpyAsync(ix->d_cl1, lv.meta.data(), lv.meta.size() * sizeof(DevCluster), cudaMemcpyHostToDevice,
+                              st));
+    ix->reg_dirty = true;
+    return PDXG_OK;
+}
+
+int enable_maintenance(pdxg_index* ix, const char* op) {
+    if (ix->maint) return PDXG_OK;
+    if (!ix->tree)
+        return fail(PDXG_ERR_UNSUPPORTED, std::string(op) + " is not implemented in PDXIndex. Use PDXTreeIndex instead.");
+    HostLevel& lv = ix->l1;
+    for (uint32_t c : ix->rid_cluster)
+        if (c == kNoCluster) return fail(PDXG_ERR_UNSUPPORTED, "the index's row ids are not 0 .. n - 1");
+    cudaStream_t st = ix->stream;
+    auto M = std::make_unique<Maint>();
+    const size_t n1 = lv.meta.size();
+    M->cl.resize(n1);
+    std::vector<DevCluster> meta(lv.meta);
+    uint64_t off = 0;
+    for (size_t c = 0; c < n1; ++c) {
+        MaintCluster& K = M->cl[c];
+        const uint32_t n = lv.n[c];
+        K.num_embeddings = K.used = n;
+        K.max_cap = std::max({lv.max_cap[c], n, 1u});
+        K.min_cap = static_cast<uint32_t>(static_cast<float>(n) * 0.5f);  // MIN_CAPACITY_THRESHOLD
+        K.indices.assign(lv.ids.begin() + lv.ids_start[c], lv.ids.begin() + lv.ids_start[c] + n);
+        off = align_up(off, 256);
+        place_cluster(lv, meta[c], off, slot_stride(K.max_cap));
+        off += cluster_block_bytes(lv, meta[c].n_pad);
+        M->live += n;
+    }
+    const uint64_t l1_bytes = align_up(off, 256);
+    const uint64_t l0_bytes = ix->arena_bytes - ix->l0_start;
+    const uint64_t used = l1_bytes + l0_bytes;
+    const uint64_t cap = used + std::max<uint64_t>(used / 4, 64ull << 20);
+    PDXG_CUDA(cudaDeviceSynchronize());  // searches in flight read the current arena
+    uint8_t* arena = nullptr;
+    PDXG_CUDA(cudaMalloc(&arena, cap));
+    auto undo = [&](cudaError_t e) {
+        cudaFree(arena);
+        return fail(PDXG_ERR_CUDA, std::string("maintenance layout: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaMemsetAsync(arena, 0, cap, st);
+    for (size_t c = 0; c < n1 && e == cudaSuccess; ++c)
+        e = copy_cluster_slots(lv, arena, meta[c], ix->arena, lv.meta[c], lv.n[c], st);
+    if (e == cudaSuccess && l0_bytes)
+        e = cudaMemcpyAsync(arena + l1_bytes, ix->arena + ix->l0_start, l0_bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return undo(e);
+    std::vector<DevCluster> meta0(ix->l0.meta);
+    for (DevCluster& m : meta0) {
+        m.vert_off = m.vert_off - ix->l0_start + l1_bytes;
+        m.hor_off = m.hor_off - ix->l0_start + l1_bytes;
+        m.ids_off = m.ids_off - ix->l0_start + l1_bytes;
+    }
+    if (!meta0.empty())
+        e = cudaMemcpyAsync(ix->d_cl0, meta0.data(), meta0.size() * sizeof(DevCluster), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return undo(e);
+    g_alloc_gen.fetch_add(1);
+    cudaFree(ix->arena);
+    ix->arena = arena;
+    ix->arena_bytes = used;
+    ix->l0_start = l1_bytes;
+    ix->l0.meta = meta0;
+    lv.meta = meta;
+    for (size_t c = 0; c < n1; ++c) lv.max_cap[c] = M->cl[c].max_cap;
+    M->arena_cap = cap;
+    M->rid_cap = ix->rid_cluster.size();
+    ix->maint = std::move(M);
+    if (int rc = relayout_bitmaps(ix, st)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+// The arena holds at least `need` bytes (the whole arena moves when it grows).
+int reserve_arena(pdxg_index* ix, uint64_t need, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    if (need <= M.arena_cap) return PDXG_OK;
+    const uint64_t cap = std::max(need + (need >> 2), M.arena_cap * 2);
+    uint8_t* arena = nullptr;
+    PDXG_CUDA(cudaMalloc(&arena, cap));
+    cudaError_t e = cudaMemsetAsync(arena, 0, cap, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(arena, ix->arena, ix->arena_bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(arena);
+        return fail(PDXG_ERR_CUDA, std::string("cannot grow the arena: ") + cudaGetErrorString(e));
+    }
+    g_alloc_gen.fetch_add(1);
+    cudaFree(ix->arena);
+    ix->arena = arena;
+    M.arena_cap = cap;
+    return PDXG_OK;
+}
+
+// In place of SplitCluster (index.hpp:1314-1610): the cluster's capacity grows to
+// max(uint32(1.3 used), 256) slots and its block moves to a fresh region of that stride.
+int grow_cluster(pdxg_index* ix, uint32_t c, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    MaintCluster& K = M.cl[c];
+    HostLevel& lv = ix->l1;
+    uint32_t cap = std::max<uint32_t>(static_cast<uint32_t>(static_cast<float>(K.used) * 1.3f), 256u);
+    if (cap <= K.used) cap = K.used + 1;
+    const uint32_t np = slot_stride(cap);
+    if (np != lv.meta[c].n_pad) {
+        const uint64_t off = align_up(ix->arena_bytes, 256);
+        const uint64_t bytes = cluster_block_bytes(lv, np);
+        if (int rc = reserve_arena(ix, off + bytes, st)) return rc;
+        DevCluster nm = lv.meta[c];
+        place_cluster(lv, nm, off, np);
+        PDXG_CUDA(copy_cluster_slots(lv, ix->arena, nm, ix->arena, lv.meta[c], K.used, st));
+        lv.meta[c] = nm;
+        ix->arena_bytes = off + bytes;
+        K.max_cap = cap;
+        lv.max_cap[c] = cap;
+        if (int rc = relayout_bitmaps(ix, st)) return rc;
+    } else {
+        K.max_cap = cap;
+        lv.max_cap[c] = cap;
+    }
+    ++M.grown;
+    return PDXG_OK;
+}
+
+// Cluster::CompactCluster (cluster.hpp:260-294) with the row-id map updates of
+// CheckClusterHealth / Save (index.hpp:1245-1248, 484-490).
+int compact_cluster(pdxg_index* ix, uint32_t c, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    MaintCluster& K = M.cl[c];
+    if (K.tombstones.empty()) return PDXG_OK;
+    const DevCluster m = ix->l1.meta[c];
+    auto drain_tail = [&]() -> int {
+        while (K.used > 0 && K.tombstones.count(K.used - 1)) {
+            K.tombstones.erase(K.used - 1);
+            if (int rc = set_tombstone_bit(ix, c, K.used - 1, false, st)) return rc;
+            K.indices[K.used - 1] = 0;
+            --K.used;
+        }
+        return PDXG_OK;
+    };
+    if (int rc = drain_tail()) return rc;
+    while (!K.tombstones.empty()) {
+        auto it = K.tombstones.begin();  // PopTombstone
+        const uint32_t t = *it;
+        K.tombstones.erase(it);
+        if (int rc = set_tombstone_bit(ix, c, t, false, st)) return rc;
+        const uint32_t last = K.used - 1;
+        PDXG_CUDA(move_slot(ix->l1, ix->arena, m, last, t, st));
+        K.indices[t] = K.indices[last];
+        ix->rid_pos[K.indices[t]] = t;
+        if (int rc = upload_row_map(ix, K.indices[t], st)) return rc;
+        K.indices[last] = 0;
+        --K.used;
+        if (int rc = drain_tail()) return rc;
+    }
+    K.indices.resize(K.used);
+    return sync_cluster(ix, c, st);
+}
+
+// CheckClusterHealth (index.hpp:1241-1255) with the split / merge substitutes above.
+int check_cluster_health(pdxg_index* ix, uint32_t c, cudaStream_t st) {
+    Maint& M = *ix->maint;
+    MaintCluster& K = M.cl[c];
+    if (K.used == K.max_cap) {
+        if (K.num_embeddings < K.used) {
+            ++M.compactions;
+            return compact_cluster(ix, c, st);
+        }
+        return grow_cluster(ix, c, st);
+    }
+    if (K.num_embeddings <= K.min_cap) ++M.merges_deferred;
+    return PDXG_OK;
+}
+
+// The nearest L1 cluster of a prepared row: the top-level search of PDXTreeIndex::Append
+// (index.hpp:597-607), k = 1 over max(1, n_L0 / 8) meso clusters, in the per-query top-level kernel.
+int nearest_l1_cluster(pdxg_index* ix, const float* d_row, uint32_t& c1, cudaStream_t st) {
+    Workspace& w = ix->ws;
+    const uint32_t top = std::max<uint32_t>(1u, (uint32_t)ix->l0.meta.size() / 8);
+    Launch L;
+    int rc = plan_search(ix, 1, 1, 0, false, L, 1, top);
+    if (rc) return rc;
+    L.p.queries = d_row;
+    const uint32_t mode = ix->top_mode;
+    ix->top_mode = 2;
+    rc = run_top_level(ix, w, d_row, 1, L, st);
+    ix->top_mode = mode;
+    if (rc) return rc;
+    if (!L.p.q_order) return fail(PDXG_ERR_CAPACITY, "top-level kernel does not fit this index");
+    uint32_t h[2] = {0, 0};
+    PDXG_CUDA(cudaMemcpyAsync(&h[0], L.p.q_order, 4, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaMemcpyAsync(&h[1], L.p.q_order_count, 4, cudaMemcpyDeviceToHost, st));
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    if (h[1] == 0 || h[0] >= ix->l1.meta.size()) return fail(PDXG_ERR_FORMAT, "Append: no L1 cluster found");
+    c1 = h[0];
+    return PDXG_OK;
+}
+
+int append_impl(pdxg_index* ix, uint64_t row_id, const float* embedding, bool transformed) {
+    Maint& M = *ix->maint;
+    if (row_id != ix->rid_cluster.size())
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "Append: row_id " + std::to_string(row_id) +
+                                                   " is not sequential (expected " +
+                                                   std::to_string(ix->rid_cluster.size()) + ")");
+    if (row_id >= 0xFFFFFFFFull) return fail(PDXG_ERR_CAPACITY, "Append: row ids are 32-bit");
+    cudaStream_t st = ix->stream;
+    Workspace& w = ix->ws;
+    const uint32_t d = ix->d;
+    if (int rc = ensure_ws(ix, w, 1, 1)) return rc;
+    PDXG_CUDA(cudaMemcpyAsync(w.d_q, embedding, (size_t)d * 4, cudaMemcpyHostToDevice, st));
+    const float* d_row = w.d_q;
+    if (!transformed) {  // NormalizeAndRotate (index.hpp:75-97, 592-594)
+        if (int rc = prepare_dev(ix, w, w.d_q, 1, w.d_rq, st, ix->append_normalize ? 1 : 0)) return rc;
+        d_row = w.d_rq;
+    }
+    std::vector<float> row(d);
+    PDXG_CUDA(cudaMemcpyAsync(row.data(), d_row, (size_t)d * 4, cudaMemcpyDeviceToHost, st));
+    uint32_t c = 0;
+    if (int rc = nearest_l1_cluster(ix, d_row, c, st)) return rc;
+    if (int rc = check_gemm_error(w)) return rc;
+    // QuantizeAndAppend + Cluster::AppendEmbedding (index.hpp:885-896, cluster.hpp:121-146)
+    MaintCluster& K = M.cl[c];
+    uint32_t slot = K.used;
+    bool reused = false;
+    if (!K.tombstones.empty()) {
+        auto it = K.tombstones.begin();  // PopTombstone
+        slot = *it;
+        K.tombstones.erase(it);
+        reused = true;
+    }
+    if (slot >= K.max_cap) return fail(PDXG_ERR_CAPACITY, "AppendEmbedding: cluster buffer overflow");
+    const HostLevel& lv = ix->l1;
+    const uint32_t dv = lv.dv;
+    std::vector<uint32_t> vwords(lv.n_vwords, 0u);
+    std::vector<uint8_t> hrow((size_t)lv.dh * (lv.u8 ? 1 : 4));
+    if (lv.u8) {
+        // ScalarQuantizer::QuantizeEmbedding (scalar.hpp:76-94)
+        std::vector<uint8_t> qb(d);
+        for (uint32_t j = 0; j < d; ++j) {
+            const int r = static_cast<int>(std::round((row[j] - ix->base) * ix->scale));
+            qb[j] = r > 255 ? 255 : (r < 0 ? 0 : static_cast<uint8_t>(r));
+        }
+        std::memcpy(vwords.data(), qb.data(), dv);
+        std::memcpy(hrow.data(), qb.data() + dv, lv.dh);
+    } else {
+        std::memcpy(vwords.data(), row.data(), (size_t)dv * 4);
+        std::memcpy(hrow.data(), row.data() + dv, (size_t)lv.dh * 4);
+    }
+    const uint32_t rid32 = (uint32_t)row_id;
+    PDXG_CUDA(write_slot(lv, ix->arena, lv.meta[c], slot, vwords.data(), hrow.data(), &rid32, st));
+    if (reused) {
+        if (int rc = set_tombstone_bit(ix, c, slot, false, st)) return rc;
+        K.indices[slot] = rid32;
+    } else {
+        K.indices.push_back(rid32);
+        ++K.used;
+    }
+    ++K.num_embeddings;
+    ix->rid_cluster.push_back(c);
+    ix->rid_pos.push_back(slot);
+    if (int rc = grow_row_maps(ix, ix->rid_cluster.size(), st)) return rc;
+    if (int rc = upload_row_map(ix, row_id, st)) return rc;
+    ++M.live;
+    ++M.appends;
+    ix->reg_dirty = true;
+    if (int rc = sync_cluster(ix, c, st)) return rc;
+    if (int rc = check_cluster_health(ix, c, st)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+int delete_impl(pdxg_index* ix, uint64_t row_id) {
+    Maint& M = *ix->maint;
+    if (row_id >= ix->rid_cluster.size())
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "Delete: row_id " + std::to_string(row_id) + " is not in the index");
+    const uint32_t c = ix->rid_cluster[row_id];
+    if (c == kNoCluster)
+        return fail(PDXG_ERR_INVALID_ARGUMENT, "Delete: row_id " + std::to_string(row_id) + " was already deleted");
+    cudaStream_t st = ix->stream;
+    const uint32_t slot = ix->rid_pos[row_id];
+    MaintCluster& K = M.cl[c];
+    // Cluster::DeleteEmbedding (cluster.hpp:148-154): the slot keeps its data and row id
+    K.tombstones.insert(slot);
+    --K.num_embeddings;
+    if (int rc = set_tombstone_bit(ix, c, slot, true, st)) return rc;
+    ix->rid_cluster[row_id] = kNoCluster;
+    ix->rid_pos[row_id] = kNoCluster;
+    if (int rc = upload_row_map(ix, row_id, st)) return rc;
+    --M.live;
+    ++M.deletes;
+    ix->reg_dirty = true;
+    if (int rc = sync_cluster(ix, c, st)) return rc;
+    if (int rc = check_cluster_health(ix, c, st)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    return PDXG_OK;
+}
+
+}  // namespace
+
+// Save compacts every cluster first (index.hpp:484-494) and writes the ids of the used slots.
+int maint_prepare_save(pdxg_index* ix) {
+    if (!ix->maint) return PDXG_OK;
+    cudaStream_t st = ix->stream;
+    PDXG_CUDA(cudaDeviceSynchronize());
+    for (uint32_t c = 0; c < ix->maint->cl.size(); ++c)
+        if (int rc = compact_cluster(ix, c, st)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(st));
+    HostLevel& lv = ix->l1;
+    lv.total_vectors = 0;
+    for (size_t c = 0; c < lv.meta.size(); ++c) {
+        lv.ids_start[c] = lv.total_vectors;
+        lv.total_vectors += ix->maint->cl[c].used;
+    }
+    lv.ids_start[lv.meta.size()] = lv.total_vectors;
+    lv.ids.resize(lv.total_vectors);
+    for (size_t c = 0; c < lv.meta.size(); ++c) {
+        const auto& ind = ix->maint->cl[c].indices;
+        std::copy(ind.begin(), ind.end(), lv.ids.begin() + lv.ids_start[c]);
+    }
+    g_alloc_gen.fetch_add(1);
+    ix->reg_dirty = true;
+    return PDXG_OK;
+}
+
+// Registered filters after Append / Delete moved slots: every bitmap rebuilt from its row ids in
+// the current layout. Called with reg_mu held.
+int refresh_registered_filters(pdxg_index* ix) {
+    if (!ix->reg_dirty) return PDXG_OK;
+    const uint32_t words = ix->l1.sel_words;
+    const uint32_t n1 = (uint32_t)ix->l1.meta.size();
+    if (ix->reg_cap) {
+        PDXG_CUDA(cudaDeviceSynchronize());  // batches in flight read the pool
+        uint32_t* sel = nullptr;
+        PDXG_CUDA(cudaMalloc(&sel, (size_t)ix->reg_cap * std::max(words, 1u) * 4));
+        g_alloc_gen.fetch_add(1);
+        cudaFree(ix->d_reg_sel);
+        ix->d_reg_sel = sel;
+        std::vector<uint32_t> bits(words), pass(n1);
+        for (uint32_t slot = 0; slot < ix->reg_cap; ++slot) {
+            if (!ix->reg_used[slot]) continue;
+            std::fill(bits.begin(), bits.end(), 0u);
+            std::fill(pass.begin(), pass.end(), 0u);
+            const auto& rows = ix->reg_rows[slot];
+            build_filter(ix, rows.data(), rows.size(), bits.data(), pass.data());
+            PDXG_CUDA(cudaMemcpy(ix->d_reg_sel + (size_t)slot * words, bits.data(), (size_t)words * 4,
+                                 cudaMemcpyHostToDevice));
+            PDXG_CUDA(cudaMemcpy(ix->d_reg_pass + (size_t)slot * n1, pass.data(), (size_t)n1 * 4,
+                                 cudaMemcpyHostToDevice));
+        }
+    }
+    ix->reg_dirty = false;
+    return PDXG_OK;
+}
+
+extern "C" {
+
+int pdxg_append(pdxg_index* ix, uint64_t row_id, const float* embedding, uint32_t flags) {
+    if (int rc = check_index(ix)) return rc;
+    if (!embedding) return fail(PDXG_ERR_INVALID_ARGUMENT, "embedding is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    if (int rc = enable_maintenance(ix, "Append")) return rc;
+    g_alloc_gen.fetch_add(1);  // captured searches hold the old cluster layout
+    PDXG_CUDA(cudaDeviceSynchronize());  // searches in flight read the slots being changed
+    return append_impl(ix, row_id, embedding, (flags & PDXG_QUERY_TRANSFORMED) != 0);
+}
+
+int pdxg_delete(pdxg_index* ix, uint64_t row_id) {
+    if (int rc = check_index(ix)) return rc;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    if (int rc = enable_maintenance(ix, "Delete")) return rc;
+    g_alloc_gen.fetch_add(1);
+    PDXG_CUDA(cudaDeviceSynchronize());  // searches in flight read the slots being changed
+    return delete_impl(ix, row_id);
+}
+
+int pdxg_set_append_normalization(pdxg_index* ix, int normalize) {
+    if (int rc = check_index(ix)) return rc;
+    ix->append_normalize = normalize != 0;
+    return PDXG_OK;
+}
+
+int pdxg_maintenance_stats(const pdxg_index* ix, uint64_t out[6]) {
+    if (int rc = check_index(ix)) return rc;
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    const Maint* M = ix->maint.get();
+    out[0] = M ? M->appends : 0;
+    out[1] = M ? M->deletes : 0;
+    out[2] = M ? M->compactions : 0;
+    out[3] = M ? M->grown : 0;
+    out[4] = M ? M->merges_deferred : 0;
+    out[5] = M ? M->n_tomb : 0;
     return PDXG_OK;
 }
 

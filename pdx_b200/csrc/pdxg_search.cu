@@ -59,8 +59,9 @@ __device__ __forceinline__ uint32_t sqdiff4(uint32_t a, uint32_t b, uint32_t acc
 }
 
 // ------------------------------------------------------------------------------------------
-// Per-level search state and operations (T threads, one query).
-template <int T, bool U8>
+// Per-level search state and operations (T threads, one query). TOMB: the level may hold
+// tombstoned slots (Append / Delete); the instantiations without it are the read-only scan.
+template <int T, bool U8, bool TOMB = false>
 struct LevelOps {
     static constexpr bool u8 = U8;
     const SearchParams& p;
@@ -113,6 +114,21 @@ struct LevelOps {
         if (!fsel) return true;
         const uint32_t* bits = fsel + c.sel_word;
         return (__ldg(bits + (v >> 5)) >> (v & 31)) & 1u;
+    }
+    // Cluster with tombstoned slots (uniform across the block).
+    __device__ __forceinline__ bool has_tombstones(const DevCluster& c) const { return TOMB && c.live < c.n; }
+    __device__ __forceinline__ bool tombstone(const DevCluster& c, uint32_t v) const {
+        return (__ldg(lv.tomb + c.sel_word + (v >> 5)) >> (v & 31)) & 1u;
+    }
+    // MaskDistancesWithTombstones (searcher.hpp:169-179): the raw distance of every tombstoned
+    // slot becomes the mask value (from_zero: every other slot becomes 0).
+    __device__ void mask_tombstones(const DevCluster& c, bool from_zero) {
+        const uint32_t mask = mask_raw();
+        for (uint32_t v = threadIdx.x; v < c.n; v += T) {
+            if (tombstone(c, v)) sh.dist[v] = mask;
+            else if (from_zero) sh.dist[v] = 0u;
+        }
+        __syncthreads();
     }
     // Algorithmic-traffic accounting (only when p.stats is set; values are block-uniform).
     __device__ __forceinline__ void count_bytes(unsigned long long b, Phase ph) const {
@@ -437,6 +453,7 @@ struct LevelOps {
         vertical_all(c, 0, lv.dv, false, 0);
         __syncthreads();
         for (uint32_t b = 0; b < lv.n_hblocks; ++b) horizontal(c, b, c.n, true);
+        if (has_tombstones(c)) mask_tombstones(c, false);
         uint32_t m = k - s.hsize;
         if (m > c.n) m = c.n;
         push_smallest(c, m);
@@ -449,6 +466,7 @@ struct LevelOps {
         const uint32_t* src = p.start_dist + (size_t)pre_row * p.start_stride;
         for (uint32_t v = threadIdx.x; v < c.n; v += T) sh.dist[v] = __ldg(src + v);
         __syncthreads();
+        if (has_tombstones(c)) mask_tombstones(c, false);
         uint32_t m = k - s.hsize;
         if (m > c.n) m = c.n;
         push_smallest(c, m);
@@ -495,6 +513,9 @@ struct LevelOps {
             skip_warmup = pct < (1.0f - kSelectivity);
         }
         bool bits_ready = false;  // sh.bits holds the vectors below the bound at `cur`
+        // tombstoned slots (unfiltered; a filter never selects them) start the warmup at the
+        // mask value and are reset to it before the survivors are taken (searcher.hpp:393, 453)
+        if (!fsel && has_tombstones(c)) mask_tombstones(c, true);
         if (!skip_warmup) {
             // Warmup (searcher.hpp:374-435); the first step starts the distances from 0
             const uint32_t needed = (uint32_t)ceilf(__fmul_rn(kSelectivity, (float)n));
@@ -504,11 +525,15 @@ struct LevelOps {
                 if (last > lv.dv) last = lv.dv;
                 const uint32_t thr = thr_raw(last);
                 count_bytes((unsigned long long)n * (last - cur) * kElem, kWarmup);
-                n_pruned = vertical_all(c, cur, last, true, thr, cur == 0 && !fsel);  // ends with a barrier
+                n_pruned = vertical_all(c, cur, last, true, thr, cur == 0 && !fsel && !has_tombstones(c));  // ends with a barrier
                 cur = last;
                 ++step;
                 bits_ready = !fsel;
             }
+        }
+        if (!fsel && has_tombstones(c)) {
+            mask_tombstones(c, false);
+            bits_ready = false;
         }
         // Prune (searcher.hpp:437-540): the vectors below the bound at the warmup's last
         // checkpoint, in position order
@@ -685,7 +710,7 @@ struct LevelOps {
                 passing = __ldg(fpass + cidx);
                 if (passing == 0) continue;
             }
-            if (c.n == 0) continue;
+            if ((TOMB ? c.live : c.n) == 0) continue;  // num_embeddings == 0 (searcher.hpp:662)
             if (p.stats && threadIdx.x == 0) s.visits += 1;
             if (s.hsize < k) {
                 long long t0 = 0;
@@ -772,7 +797,7 @@ __device__ void prepare_query(const SearchParams& p, Shared& sh, uint32_t q) {
     }
 }
 
-template <bool U8, int T>
+template <bool U8, int T, bool TOMB>
 __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ Scalars s;
@@ -842,7 +867,7 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
             s.cycles[0] += (unsigned long long)(now - t_q0);
             t_q0 = now;
         }
-        LevelOps<T, U8> ops(p, p.l1, sh, s, filter);
+        LevelOps<T, U8, TOMB> ops(p, p.l1, sh, s, filter);
         if (U8 && p.start_row && filter == -1) {
             ops.pre_row = __ldg(p.start_row + q);
             ops.pre_cluster = __ldg(p.start_first + q);
@@ -961,7 +986,7 @@ int top_level_occupancy(size_t smem) {
 // ------------------------------------------------------------------------------------------
 template <bool U8, int T>
 static cudaError_t launch_t(const SearchParams& p, int grid, cudaStream_t st) {
-    auto kern = search_kernel<U8, T>;
+    auto kern = p.l1.tomb ? search_kernel<U8, T, true> : search_kernel<U8, T, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)p.smem_total);
     if (e != cudaSuccess) return e;
@@ -972,8 +997,8 @@ static cudaError_t launch_t(const SearchParams& p, int grid, cudaStream_t st) {
 template <bool U8, int T>
 static int occupancy_u(size_t smem) {
     int blocks = 0;
-    cudaFuncSetAttribute(search_kernel<U8, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, search_kernel<U8, T>, T, smem);
+    cudaFuncSetAttribute(search_kernel<U8, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, search_kernel<U8, T, false>, T, smem);
     return blocks;
 }
 template <int T>

@@ -35,7 +35,7 @@ __global__ void start_count_kernel(const __grid_constant__ StartParams sp) {
     const uint32_t* ord = sp.q_order + (size_t)q * sp.q_order_stride;
     for (uint32_t i = 0; i < cnt; ++i) {
         const uint32_t c = ord[i];
-        if (sp.l1.clusters[c].n == 0) continue;
+        if (sp.l1.clusters[c].live == 0) continue;  // num_embeddings == 0 (searcher.hpp:662)
         sp.first_cl[q] = c;
         sp.slot_of[q] = atomicAdd(sp.cl_count + c, 1u);
         return;
