@@ -130,6 +130,100 @@ def run_build(name, cfg, device):
         "nprobe": cfg["nprobe"], "data": "synthetic"}), flush=True)
 
 
+def run_maintenance(args, cfg, path, gm, device, n_ops=2000, n_ref_ops=200):
+    """PDXTreeIndex::Append / Delete through the public API on the loaded workload index (host rows,
+    wall clock per call, the device synchronized on both sides), then the device search of the
+    workload's batch over the index with the tombstones left behind. The reference's own Append /
+    Delete (oracle/_ref: its Cluster code, its rotation) run on the host beside it on a bounded
+    sample. Rows are normalized on the host: a loaded index appends rows as given (LoadPDXIndex's
+    default config does not normalize)."""
+    import torch
+    from pdx_b200 import compiled
+    from pdx_b200.builder import normalize_rows
+    if "tree" not in cfg["itype"]:
+        raise SystemExit("--maintenance needs a tree workload")
+    n = cfg["n"]
+    rows = normalize_rows(gm.sample(n_ops, 21)) if cfg["normalize"] else gm.sample(n_ops, 21)
+    victims = np.random.default_rng(5).choice(n, n_ops, replace=False)
+    ix = compiled.load_index(path, device=torch.cuda.current_device())
+    ix.set_nprobe(cfg["nprobe"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ix.append(n, rows[0])  # first call lays the clusters out at their capacity strides
+    torch.cuda.synchronize()
+    t_first = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for i in range(1, n_ops):
+        ix.append(n + i, rows[i])
+    torch.cuda.synchronize()
+    t_app = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for v in victims:
+        ix.delete(int(v))
+    torch.cuda.synchronize()
+    t_del = time.perf_counter() - t0
+    # batched appends (one rotation and top-level search per 4,096 rows)
+    n_batch = 50_000
+    brows = normalize_rows(gm.sample(n_batch, 22)) if cfg["normalize"] else gm.sample(n_batch, 22)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for a in range(0, n_batch, 4096):
+        ix.append_batch(n + n_ops + a, brows[a:a + 4096])
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    st = ix.maintenance_stats()
+    # search with tombstones (the scan's tombstone-masking instantiation)
+    nq, k = cfg["nq"], cfg["k"]
+    q = torch.from_numpy(gm.sample(nq, 1)).to(device)
+    ids = torch.empty((nq, k), dtype=torch.int32, device=device)
+    ds = torch.empty((nq, k), dtype=torch.float32, device=device)
+    cnt = torch.empty(nq, dtype=torch.int32, device=device)
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    for _ in range(3):
+        ix.search_device(q.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(), stream=sp)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    reps = 10
+    for _ in range(reps):
+        ix.search_device(q.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(), stream=sp)
+    b.record(stream)
+    torch.cuda.synchronize()
+    qps = nq * reps / (a.elapsed_time(b) / 1e3)
+    deleted = set(int(v) for v in victims)
+    found_deleted = int(np.isin(ids.cpu().numpy().view(np.uint32), list(deleted)).sum())
+    ref_line = None
+    try:
+        from oracle.oracle import Reference
+        if Reference.available():
+            ref = Reference(path)
+            t0 = time.perf_counter()
+            for i in range(n_ref_ops):
+                ref.append(n + i, rows[i])
+            r_app = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            for v in victims[:n_ref_ops]:
+                ref.delete(int(v))
+            r_del = time.perf_counter() - t0
+            ref.close()
+            ref_line = {"appends_per_s": round(n_ref_ops / r_app, 1), "deletes_per_s": round(n_ref_ops / r_del, 1),
+                        "cores": 1, "kind": "reference", "sample": f"first {n_ref_ops} appends and deletes"}
+    except Exception as e:  # the CPU baseline is reported, never required
+        ref_line = {"unavailable": str(e)[:200]}
+    print(json.dumps({
+        "metric": "Append / Delete throughput on the loaded tree index (host rows, one call each)",
+        "value": round((n_ops - 1) / t_app, 1), "unit": "appends/s", "higher_is_better": True,
+        "deletes_per_s": round(n_ops / t_del, 1), "first_append_s": round(t_first, 3),
+        "batch_appends_per_s": round(n_batch / t_batch, 1), "batch_rows": 4096,
+        "maintenance_stats": st,
+        "search_after": {"qps_device": round(qps, 1), "batch_queries": nq, "nprobe": cfg["nprobe"], "k": k,
+                         "deleted_rows_returned": found_deleted},
+        "config": {"workload": cfg.get("dataset", args.config), "index": cfg["itype"], "n": n, "d": cfg["d"],
+                   "ops": n_ops},
+        "cpu_baseline": ref_line, "data": "synthetic"}), flush=True)
+
+
 def ground_truth(X, Q, k, device, normalize):
     """Exact FP64 L2 neighbours in the original (normalized when the index is) space."""
     import torch
@@ -276,6 +370,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrivals per rate (seconds)")
     ap.add_argument("--build", action="store_true",
                     help="time the native GPU index build of the workload's data and exit")
+    ap.add_argument("--maintenance", action="store_true",
+                    help="time Append / Delete on the workload's tree index, then search with tombstones")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -313,6 +409,13 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, cfg, path, gm, gt, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    if args.maintenance:
+        if rank == 0:
+            run_maintenance(args, cfg, path, gm, device)
         if world > 1:
             dist.destroy_process_group()
         return

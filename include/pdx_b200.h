@@ -139,6 +139,13 @@ int pdxg_save(pdxg_index* index, const char* path);
  * ("Append is not implemented in PDXIndex", index.hpp:405-407). Not concurrent with searches. */
 int pdxg_append(pdxg_index* index, uint64_t row_id, const float* embedding, uint32_t flags);
 
+/* n appends of rows first_row_id, first_row_id + 1, ... (n x d floats, host memory, row-major),
+ * with the results of n pdxg_append calls in that order: a row's cluster comes from the top-level
+ * search over the meso level, which appends never change, so one batched rotation and top-level
+ * search serve the batch, and the slots and health checks follow row by row. */
+int pdxg_append_batch(pdxg_index* index, uint64_t first_row_id, uint32_t n, const float* embeddings,
+                      uint32_t flags);
+
 /* Replaces PDXTreeIndex::Delete (index.hpp:619-638) and PDXIndex.delete (python/lib.cpp:52):
  * tombstones the row's slot. PDXG_ERR_INVALID_ARGUMENT for a row never appended or already
  * deleted. After Append and Delete the cluster health check of index.hpp:1241-1255 runs: a full

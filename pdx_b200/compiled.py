@@ -94,6 +94,7 @@ def library() -> C.CDLL:
         fn("pdxg_filter_register", C.c_int, vp, vp, C.c_uint64, C.POINTER(C.c_int32))
         fn("pdxg_filter_release", C.c_int, vp, C.c_int32)
         fn("pdxg_append", C.c_int, vp, C.c_uint64, _f32p, C.c_uint32)
+        fn("pdxg_append_batch", C.c_int, vp, C.c_uint64, C.c_uint32, _f32p, C.c_uint32)
         fn("pdxg_delete", C.c_int, vp, C.c_uint64)
         fn("pdxg_set_append_normalization", C.c_int, vp, C.c_int)
         fn("pdxg_maintenance_stats", C.c_int, vp, _u64p)
@@ -483,6 +484,19 @@ class PDXIndex:
             raise ValueError(f"Append: row_id {row_id} is not sequential")
         _check(library().pdxg_append(self._handle().ptr, int(row_id), e,
                                      PDXG_QUERY_TRANSFORMED if transformed else 0))
+
+    def append_batch(self, first_row_id: int, embeddings: np.ndarray, transformed: bool = False) -> None:
+        """Rows first_row_id, first_row_id + 1, ... appended in order (extension): the results of
+        one append() per row, with one rotation and top-level search for the batch."""
+        if self._type in ("pdx_f32", "pdx_u8"):
+            raise RuntimeError("Append is not implemented in PDXIndex. Use PDXTreeIndex instead.")
+        e = np.ascontiguousarray(embeddings, dtype=np.float32)
+        if e.ndim != 2 or e.shape[1] != self._d:
+            raise ValueError(f"embeddings must be n x {self._d}")
+        if first_row_id < 0:
+            raise ValueError(f"Append: row_id {first_row_id} is not sequential")
+        _check(library().pdxg_append_batch(self._handle().ptr, int(first_row_id), e.shape[0], e,
+                                           PDXG_QUERY_TRANSFORMED if transformed else 0))
 
     def delete(self, row_id: int) -> None:
         """PDXTreeIndex::Delete (index.hpp:619-638)."""

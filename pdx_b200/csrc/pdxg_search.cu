@@ -20,6 +20,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "pdxg_block.cuh"
 #include "pdxg_common.cuh"
 
@@ -976,11 +980,35 @@ cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-int top_level_occupancy(size_t smem) {
-    int blocks = 0;
-    cudaFuncSetAttribute(top_level_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, top_level_kernel<64>, 64, smem);
+// Resident CTAs per SM, remembered per (device, kernel form, threads, shared memory): the planner
+// asks for every search, and a single-row Append pays the driver query otherwise.
+template <class F>
+static int cached_occupancy(int kind, int threads, size_t smem, F query) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, kind, threads, smem);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    const int blocks = query();
+    if (blocks > 0) {
+        std::lock_guard<std::mutex> lock(mu);
+        cache[key] = blocks;
+    }
     return blocks;
+}
+
+int top_level_occupancy(size_t smem) {
+    return cached_occupancy(-1, 64, smem, [&] {
+        int blocks = 0;
+        cudaFuncSetAttribute(top_level_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, top_level_kernel<64>, 64, smem);
+        return blocks;
+    });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1007,13 +1035,15 @@ static int occupancy_t(bool u8, size_t smem) {
 }
 
 int search_occupancy(bool u8, int threads, size_t smem) {
-    switch (threads) {
-    case 64: return occupancy_t<64>(u8, smem);
-    case 128: return occupancy_t<128>(u8, smem);
-    case 256: return occupancy_t<256>(u8, smem);
-    case 512: return occupancy_t<512>(u8, smem);
-    default: return 0;
-    }
+    return cached_occupancy(u8 ? 1 : 0, threads, smem, [&] {
+        switch (threads) {
+        case 64: return occupancy_t<64>(u8, smem);
+        case 128: return occupancy_t<128>(u8, smem);
+        case 256: return occupancy_t<256>(u8, smem);
+        case 512: return occupancy_t<512>(u8, smem);
+        default: return 0;
+        }
+    });
 }
 
 cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid, cudaStream_t st) {

@@ -250,3 +250,54 @@ def test_flat_index_append_is_not_implemented():
         ix = compiled.load_index(p)
         with pytest.raises(RuntimeError, match="Append is not implemented in PDXIndex"):
             ix.append(800, X[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("itype", ["pdx_tree_f32", "pdx_tree_u8"])
+def test_batch_append_equals_row_appends(ref_cls, itype):
+    """append_batch over chunks of several sizes (one crossing a capacity growth) leaves the same
+    clusters, counters and search results as one append per row, and as the oracle."""
+    from pdx_b200 import compiled
+    rng = np.random.default_rng(4)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f, gm, X = _tree_file(p, itype, seed=8)
+        n = X.shape[0]
+        rows_ix = compiled.load_index(p)
+        batch_ix = compiled.load_index(p)
+        ref = ref_cls(p)
+        new = rows_ix.prepare_queries(gm.sample(300, 6))
+        near = new[0] + rng.normal(0, 2e-3, (200, new.shape[1])).astype(np.float32)
+        rows = np.concatenate([near, new]).astype(np.float32)
+        victims = rng.choice(n, 60, replace=False)
+        for v in victims[:30]:
+            for ix in (rows_ix, batch_ix):
+                ix.delete(int(v))
+            ref.delete(int(v))
+        for i, r in enumerate(rows):
+            rows_ix.append(n + i, r, transformed=True)
+            ref.append(n + i, r, transformed=True)
+        a = 0
+        for size in (1, 7, 250, len(rows)):
+            b = min(len(rows), a + size)
+            batch_ix.append_batch(n + a, rows[a:b], transformed=True)
+            a = b
+            if a == len(rows):
+                break
+        for v in victims[30:]:
+            for ix in (rows_ix, batch_ix):
+                ix.delete(int(v))
+            ref.delete(int(v))
+        assert rows_ix.maintenance_stats() == batch_ix.maintenance_stats()
+        assert batch_ix.maintenance_stats()["capacity_growths"] >= 1
+        _same_clusters(batch_ix, ref)
+        _same_clusters(rows_ix, ref)
+        Q = batch_ix.prepare_queries(gm.sample(16, 9))
+        for ix in (rows_ix, batch_ix):
+            ix.set_nprobe(0)
+        ref.set_nprobe(0)
+        _compare(batch_ix, ref, Q, 10, ctx=f"{itype} batch")
+        _compare(rows_ix, ref, Q, 10, ctx=f"{itype} rows")
+        with pytest.raises(ValueError, match="not sequential"):
+            batch_ix.append_batch(n, rows[:2], transformed=True)
+        ref.close()
