@@ -301,3 +301,36 @@ def test_batch_append_equals_row_appends(ref_cls, itype):
         with pytest.raises(ValueError, match="not sequential"):
             batch_ix.append_batch(n, rows[:2], transformed=True)
         ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tree_f32_d130", "tree_u8_d256"])
+def test_engine_matches_oracle_on_reference_files(ref_cls, name):
+    """The same parity on index files the reference itself wrote (golden fixtures)."""
+    from pdx_b200 import compiled
+    from tests.helpers import load_golden
+    path, queries, rotated, exp = load_golden(name)
+    ix = compiled.load_index(path)
+    ref = ref_cls(path)
+    n = ix.get_num_embeddings()
+    rng = np.random.default_rng(2)
+    live = list(range(n))
+    base = ix.prepare_queries(queries)
+    next_id = n
+    for step in range(120):
+        if rng.random() < 0.6:
+            row = (base[step % len(base)] + rng.normal(0, 0.02, base.shape[1])).astype(np.float32)
+            ix.append(next_id, row, transformed=True)
+            ref.append(next_id, row, transformed=True)
+            live.append(next_id)
+            next_id += 1
+        else:
+            v = live.pop(int(rng.integers(len(live))))
+            ix.delete(v)
+            ref.delete(v)
+    _same_clusters(ix, ref)
+    for nprobe in (0, exp["nprobe"]):
+        ix.set_nprobe(nprobe)
+        ref.set_nprobe(nprobe)
+        _compare(ix, ref, rotated, exp["k"], ctx=f"{name} nprobe {nprobe}")
+    ref.close()
