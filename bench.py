@@ -598,6 +598,16 @@ def main():
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(statistics.mean(e2e_times), device)
     e2e_value = whole_job_qps(nq, 1, world, e2e_s * 1e3)
+    # the query upload alone (pinned host -> device, the same bytes), to explain e2e vs value
+    h2d_ms = []
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        q_dev.copy_(q_pin, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        h2d_ms.append(a.elapsed_time(b))
+    h2d_gbs = nq * d * 4 / (min(h2d_ms) * 1e-3) / 1e9
 
     # ---- CPU baseline: the reference's own search on this host, bounded sample
     cpu = None
@@ -662,7 +672,9 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
                     "h2d_bytes_per_step": nq * d * 4,
-                    "d2h_bytes_per_step": nq * k * 8 + nq * 4},
+                    "d2h_bytes_per_step": nq * k * 8 + nq * 4,
+                    "h2d_gbs_measured": round(h2d_gbs, 1),
+                    "h2d_ms_per_step": round(min(h2d_ms), 3)},
             # per step: query preparation + [tree top level] + scan, as counted by the engine
             "gpu_launches": args.steps * launches_per_step,
             "clocks": clocks,

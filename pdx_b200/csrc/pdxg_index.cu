@@ -28,8 +28,8 @@ cudaError_t launch_search(const SearchParams& p, bool u8, int threads, int grid,
 int search_occupancy(bool u8, int threads, size_t smem);
 cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, const float* rotation,
                                    bool normalize, float* norms_ws, float* out, cudaStream_t st);
-cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st);
-int top_level_occupancy(size_t smem);
+cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st, int threads);
+int top_level_occupancy(size_t smem, int threads);
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
                                    cudaStream_t st);
 cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t st);
@@ -1051,10 +1051,11 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     tp.q_order_stride = k1;
     tp.queue = w.d_queue + 2;
     PDXG_CUDA(cudaMemsetAsync(tp.queue, 0, sizeof(uint32_t), st));
-    const int occ = top_level_occupancy(off);
+    const int threads = nq <= (uint32_t)ix->num_sms ? 256 : 64;
+    const int occ = top_level_occupancy(off, threads);
     if (occ <= 0) return fail(PDXG_ERR_CAPACITY, "top-level kernel cannot be resident");
     const int grid = (int)std::min<uint64_t>(nq, (uint64_t)occ * ix->num_sms);
-    PDXG_CUDA(launch_top_level(tp, grid, st));
+    PDXG_CUDA(launch_top_level(tp, grid, st, threads));
     L.top_launches = 1;
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
@@ -1423,8 +1424,14 @@ int search_host_pipelined(pdxg_index* ix, const float* queries, uint32_t nq, uin
     if (!ix->copy_stream) PDXG_CUDA(cudaStreamCreateWithFlags(&ix->copy_stream, cudaStreamNonBlocking));
     for (cudaEvent_t& e : ix->chunk_ev)
         if (!e) PDXG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    const uint32_t nch = 2;  // measured on B200: 2 chunks beat 4 (the top level loses tile fill)
-    const uint32_t chunk = (nq + nch - 1) / nch;
+    // two chunks (measured on B200: more chunks cost the top level its tile fill); the first is a
+    // quarter of the batch, so that only its upload is exposed and the larger second upload
+    // overlaps the first chunk's rotation and top level (10,000 x 1024 queries: first chunk
+    // 1/8, 1/4, 1/3, 1/2 gave 2.68, 2.87, 2.80, 2.71 M queries/s end to end)
+    const uint32_t nch = 2;
+    const uint32_t first = nq >= 1024 ? (nq / 4 + 31) / 32 * 32 : nq;
+    auto chunk_off = [&](uint32_t c) { return c == 0 ? 0u : std::min(first, nq); };
+    auto chunk_len = [&](uint32_t c) { return c == 0 ? std::min(first, nq) : nq - std::min(first, nq); };
     Launch L;
     if ((rc = plan_search(ix, nq, k, 0, false, L))) return rc;
     L.p.out_ids = w.d_ids;
@@ -1440,9 +1447,8 @@ int search_host_pipelined(pdxg_index* ix, const float* queries, uint32_t nq, uin
     uint32_t launches = 1;
     bool orders = top;
     for (uint32_t c = 0; c < nch; ++c) {
-        const uint32_t off = c * chunk;
-        if (off >= nq) break;
-        const uint32_t n = std::min(chunk, nq - off);
+        const uint32_t off = chunk_off(c), n = chunk_len(c);
+        if (n == 0) break;
         PDXG_CUDA(cudaMemcpyAsync(w.d_q + (uint64_t)off * d, queries + (uint64_t)off * d, sizeof(float) * n * d,
                                   cudaMemcpyHostToDevice, ix->copy_stream));
         PDXG_CUDA(cudaEventRecord(ix->chunk_ev[c], ix->copy_stream));

@@ -972,11 +972,13 @@ __global__ void __launch_bounds__(T) top_level_kernel(const __grid_constant__ Se
     }
 }
 
-cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st) {
-    auto kern = top_level_kernel<64>;
+// 64 threads per query for batches (many CTAs per SM), 256 when a few queries have the GPU to
+// themselves (an Append, a single query): the same decisions, less latency.
+cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st, int threads) {
+    auto kern = threads == 256 ? top_level_kernel<256> : top_level_kernel<64>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_total);
     if (e != cudaSuccess) return e;
-    kern<<<grid, 64, p.smem_total, st>>>(p);
+    kern<<<grid, threads == 256 ? 256 : 64, p.smem_total, st>>>(p);
     return cudaGetLastError();
 }
 
@@ -1002,11 +1004,12 @@ static int cached_occupancy(int kind, int threads, size_t smem, F query) {
     return blocks;
 }
 
-int top_level_occupancy(size_t smem) {
-    return cached_occupancy(-1, 64, smem, [&] {
+int top_level_occupancy(size_t smem, int threads) {
+    return cached_occupancy(-1, threads, smem, [&] {
         int blocks = 0;
-        cudaFuncSetAttribute(top_level_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, top_level_kernel<64>, 64, smem);
+        auto kern = threads == 256 ? top_level_kernel<256> : top_level_kernel<64>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, threads == 256 ? 256 : 64, smem);
         return blocks;
     });
 }
