@@ -334,3 +334,52 @@ def test_engine_matches_oracle_on_reference_files(ref_cls, name):
         ref.set_nprobe(nprobe)
         _compare(ix, ref, rotated, exp["k"], ctx=f"{name} nprobe {nprobe}")
     ref.close()
+
+
+@pytest.mark.gpu
+def test_request_batches_after_maintenance(ref_cls):
+    """Serving batches (a context's pdxg_search_requests) after Append / Delete: per-request k and
+    nprobe, row-list filters and a filter registered before the changes (rebuilt from its row ids,
+    which name deleted rows and rows appended later) equal the oracle's searches."""
+    from pdx_b200 import compiled
+    from tests.test_gpu_serving import _run_requests
+    rng = np.random.default_rng(21)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f, gm, X = _tree_file(p, "pdx_tree_u8", seed=5)
+        n = X.shape[0]
+        ix = compiled.load_index(p)
+        ref = ref_cls(p)
+        ctx = compiled.Context(ix)
+        victims = rng.choice(n, 200, replace=False)
+        fl_rows = np.concatenate([victims[:40], rng.choice(n, 300, replace=False), np.arange(n, n + 60)])
+        fid = ix.register_filter(fl_rows.astype(np.uint64))
+        R = ix.prepare_queries(gm.sample(32, 4))
+        new = ix.prepare_queries(gm.sample(150, 5))
+        for i, r in enumerate(new):
+            ix.append(n + i, r, transformed=True)
+            ref.append(n + i, r, transformed=True)
+        for v in victims:
+            ix.delete(int(v))
+            ref.delete(int(v))
+        live = np.array(sorted(set(range(n + len(new))) - set(victims.tolist())), np.uint32)
+        reqs = []
+        for i in range(len(R)):
+            k = int(rng.choice((1, 10, 20)))
+            npb = int(rng.choice((0, 3, 8)))
+            kind = i % 3
+            rows = None if kind == 0 else (fid if kind == 1 else
+                                           np.sort(rng.choice(live, 250, replace=False)).astype(np.uint32))
+            reqs.append((k, npb, rows))
+        ids, ds, cnt = _run_requests(ctx, R, reqs, 20)
+        for i, (k, npb, rows) in enumerate(reqs):
+            ref.set_nprobe(npb)
+            if rows is None:
+                pi, pd = ref.search(R[i], k, transformed=True)
+            else:
+                sel = fl_rows if isinstance(rows, int) else rows
+                pi, pd = ref.filtered_search(R[i], k, sel.astype(np.uint64), transformed=True)
+            assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd, ctx=f"request {i} k={k} nprobe={npb}")
+            assert not set(ids[i, :cnt[i]].tolist()) & set(victims.tolist())
+        ctx.close()
+        ref.close()
