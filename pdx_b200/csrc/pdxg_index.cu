@@ -863,7 +863,8 @@ int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float
     if (nq == 0) return PDXG_OK;
     const uint32_t d = ix->d;
     const bool norm = normalize < 0 ? ix->normalized : normalize != 0;
-    if (allow_tc && ix->rot_tc && ix->rot_mode == 0) {
+    // up to 8 rows (a single query, an appended row): the FP32 GEMV has the shorter latency
+    if (allow_tc && ix->rot_tc && ix->rot_mode == 0 && nq > 8) {
         int rc;
         if ((rc = dev_grow(w.d_qhi, w.qhi_cap, (uint64_t)nq * d))) return rc;
         if ((rc = dev_grow(w.d_qlo, w.qlo_cap, (uint64_t)nq * d))) return rc;
@@ -1308,7 +1309,7 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         if ((rc = prepare_dev(ix, w, q, nq, w.d_rq, st))) return rc;
         qp = w.d_rq;
         // TF32 split + tensor-core GEMM, or [norms +] SIMT GEMM
-        launches += (ix->rot_tc && ix->rot_mode == 0) ? 2 : (ix->normalized ? 2 : 1);
+        launches += (ix->rot_tc && ix->rot_mode == 0 && nq > 8) ? 2 : (ix->normalized ? 2 : 1);
     }
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[1], st));
     Launch L;
@@ -1457,7 +1458,7 @@ int search_host_pipelined(pdxg_index* ix, const float* queries, uint32_t nq, uin
         if (!transformed) {
             if ((rc = prepare_dev(ix, w, qc, n, w.d_rq + (uint64_t)off * d, st))) return rc;
             qc = w.d_rq + (uint64_t)off * d;
-            launches += (ix->rot_tc && ix->rot_mode == 0) ? 2 : (ix->normalized ? 2 : 1);
+            launches += (ix->rot_tc && ix->rot_mode == 0 && n > 8) ? 2 : (ix->normalized ? 2 : 1);
         }
         if (top) {
             Launch Lc = L;

@@ -24,6 +24,56 @@ __global__ void query_norms_kernel(const float* __restrict__ q, uint32_t nq, uin
     if (lane == 0) norms[warp] = (s == 0.0f) ? 1.0f : sqrtf(s);
 }
 
+// A few rows (nq <= kGemvRows, a single query or an appended row): C[nq x d] = (A / norm) @ B
+// with 32 output columns per 1024-thread CTA, lane = column and warp = K slice (rows w, w + 32,
+// ... of B, FMA in that order, eight rows of B loaded before their FMAs); the 32 warps' partial
+// sums are then added in warp order, so the result does not depend on timing. B is read once,
+// 128 contiguous bytes per warp and row.
+constexpr uint32_t kGemvRows = 8;
+constexpr uint32_t kGemvWarps = 32;
+
+__global__ void __launch_bounds__(1024) rotate_gemv_kernel(const float* __restrict__ A,
+                                                           const float* __restrict__ norms,
+                                                           const float* __restrict__ B,
+                                                           float* __restrict__ C, uint32_t M,
+                                                           uint32_t N, uint32_t K) {
+    __shared__ float part[kGemvWarps][kGemvRows][32];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t col = blockIdx.x * 32 + lane;
+    float acc[kGemvRows];
+#pragma unroll
+    for (uint32_t r = 0; r < kGemvRows; ++r) acc[r] = 0.0f;
+    for (uint32_t i0 = warp; i0 < K; i0 += kGemvWarps * 8) {
+        float b[8];
+#pragma unroll
+        for (uint32_t t = 0; t < 8; ++t) {
+            const uint32_t i = i0 + kGemvWarps * t;
+            b[t] = (i < K && col < N) ? __ldg(B + (size_t)i * N + col) : 0.0f;
+        }
+#pragma unroll
+        for (uint32_t t = 0; t < 8; ++t) {
+            const uint32_t i = i0 + kGemvWarps * t;
+            if (i >= K) break;
+            for (uint32_t r = 0; r < M; ++r) {
+                float a = __ldg(A + (size_t)r * K + i);
+                if (norms) a = __fdiv_rn(a, __ldg(norms + r));
+                acc[r] = __fmaf_rn(a, b[t], acc[r]);
+            }
+        }
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < kGemvRows; ++r)
+        if (r < M) part[warp][r][lane] = acc[r];
+    __syncthreads();
+    if (warp == 0 && col < N) {
+        for (uint32_t r = 0; r < M; ++r) {
+            float s = part[0][r][lane];
+            for (uint32_t w = 1; w < kGemvWarps; ++w) s = __fadd_rn(s, part[w][r][lane]);
+            C[(size_t)r * N + col] = s;
+        }
+    }
+}
+
 // C[nq x d] = (A / norm)[nq x d] @ B[d x d]; 128x64 output tile per 256-thread CTA,
 // 8x4 outputs per thread, K step 16, double-buffered through shared memory.
 constexpr int RBM = 128, RBN = 64, RBK = 16;
@@ -107,6 +157,11 @@ cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, cons
         const uint32_t threads = 256;
         const uint32_t blocks = (nq * 32 + threads - 1) / threads;
         query_norms_kernel<<<blocks, threads, 0, st>>>(q, nq, d, norms_ws);
+    }
+    if (nq <= kGemvRows) {
+        rotate_gemv_kernel<<<(d + 31) / 32, 1024, 0, st>>>(q, normalize ? norms_ws : nullptr, rotation, out, nq,
+                                                           d, d);
+        return cudaGetLastError();
     }
     dim3 grid((d + RBN - 1) / RBN, (nq + RBM - 1) / RBM);
     rotate_sgemm_kernel<<<grid, 256, 0, st>>>(q, normalize ? norms_ws : nullptr, rotation, out, nq,

@@ -452,3 +452,29 @@ def test_tree_top_level_batched_edge_sizes(port_cls):
                         assert_same(ids[i, :cnt[i]], ds[i, :cnt[i]], pi, pd,
                                     ctx=f"{itype} mode={mode} nprobe={nprobe} k={k} q{i}")
             port.close()
+
+
+@pytest.mark.parametrize("d", [100, 512, 1024])
+def test_few_row_rotation_against_fp64(d):
+    """Batches of up to 8 rows rotate with the FP32 GEMV (one CTA per 32 columns, fixed order);
+    larger ones with the tensor-core or SIMT GEMM. Every size agrees with the FP64 rotation of the
+    normalized rows at FP32 rounding level (rtol 1e-5)."""
+    gm = GaussianMixture(d, 8, 0.4, seed=d, unit_norm=False)
+    X = gm.sample(1200, 0)
+    f = build_index(X, "pdx_tree_u8", num_clusters=12, num_meso_clusters=3, normalize=True, seed=2)
+    Q = gm.sample(20, 1)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f.save(p)
+        ix = compiled.load_index(p)
+        rot = np.asarray(f.rotation, np.float64)
+        Qn = Q.astype(np.float64) / np.linalg.norm(Q.astype(np.float64), axis=1, keepdims=True)
+        R64 = Qn @ rot
+        for m in (1, 3, 8, 9, 20):
+            got = ix.prepare_queries(Q[:m])
+            np.testing.assert_allclose(got, R64[:m], rtol=1e-5, atol=1e-6, err_msg=f"{m} rows")
+        # a single raw query searches like its prepared form within the rotation's rounding
+        ix.set_nprobe(0)
+        a, _, ca = ix.search_batch(Q[:1], 10)
+        b, _, cb = ix.search_batch(ix.prepare_queries(Q[:1]), 10, transformed=True)
+        assert ca[0] == cb[0] and set(a[0, :ca[0]].tolist()) == set(b[0, :cb[0]].tolist())
