@@ -337,9 +337,11 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
         const float* qs = S.q[st & 1];
         const float* xs = S.x[st & 1];
         const uint32_t row = ncp + (st - nvc);
-        // two passes of 4 queries x 2 vectors (vg + 16 h, vg + 16 h + 8)
+        // two passes of 4 queries x 2 vectors (vg + 16 h, vg + 16 h + 8); a tile with at most 16
+        // vectors left (a cluster's tail) stores nothing from the second pass, which it skips
+        const int passes = (c.n - v0 <= 16u) ? 1 : 2;
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < passes; ++h) {
             const uint32_t xo0 = (vg + 16 * h) * kRow, xo1 = (vg + 16 * h + 8) * kRow;
             double D0[4][2], D1[4][2], E0[4][2], E1[4][2];
             // lane pairs in the order they combine: (0,1) + (4,5) -> s0, s1; (2,3) + (6,7) -> s2, s3
