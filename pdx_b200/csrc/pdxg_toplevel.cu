@@ -29,6 +29,7 @@
 //      The sorted L1 visit order goes to l1_order for the search kernel.
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "pdxg_block.cuh"
@@ -284,8 +285,11 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
     };
 
     // vertical dims: one chain per (query, vector), stored at every checkpoint. Vectors
-    // 2 vg + {0, 1} and 2 vg + 16 + {0, 1}, each adjacent pair in one packed register.
-    {
+    // 2 vg + {0, 1} and 2 vg + 16 + {0, 1}, each adjacent pair in one packed register; a tile
+    // with at most 16 vectors left (a cluster's tail) runs the first half only (NB = 1), as it
+    // stores nothing from the second.
+    auto vertical = [&](auto nb_tag) {
+        constexpr int NB = decltype(nb_tag)::value;
         uint64_t acc[4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = 0ull;
@@ -303,12 +307,12 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
 #pragma unroll
                     for (int i = 0; i < 4; ++i) qv[i] = f32x2_dup(qs[(slot0 + 4 * i) * kRow + jj + u]);
 #pragma unroll
-                    for (int b = 0; b < 2; ++b)
+                    for (int b = 0; b < NB; ++b)
                         xv[b] = *reinterpret_cast<const uint64_t*>(xs + (jj + u) * kTV + 2 * vg + 16 * b);
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int b = 0; b < 2; ++b) {
+                        for (int b = 0; b < NB; ++b) {
                             const uint64_t t = f32x2_sub(qv[i], xv[b]);
                             acc[i][b] = f32x2_fma(t, t, acc[i][b]);
                         }
@@ -317,7 +321,7 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int b = 0; b < 2; ++b) {
+                        for (int b = 0; b < NB; ++b) {
                             const uint32_t v = v0 + 2 * vg + 16 * b;
                             if (slot_ok(i) && v < stride)
                                 *reinterpret_cast<uint64_t*>(out_row(i, ck) + v) = acc[i][b];
@@ -327,7 +331,10 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
             }
             __syncthreads();
         }
-    }
+    };
+    const bool tail = c.n - v0 <= 16u;
+    if (tail) vertical(std::integral_constant<int, 1>());
+    else vertical(std::integral_constant<int, 2>());
 
     // horizontal blocks: per (query, vector) the AVX2 Horizontal sum of each block. Lanes
     // (j, j + 1) of Horizontal run as one packed chain: dims j + 8 t and j + 1 + 8 t are
@@ -339,7 +346,7 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
         const uint32_t row = ncp + (st - nvc);
         // two passes of 4 queries x 2 vectors (vg + 16 h, vg + 16 h + 8); a tile with at most 16
         // vectors left (a cluster's tail) stores nothing from the second pass, which it skips
-        const int passes = (c.n - v0 <= 16u) ? 1 : 2;
+        const int passes = tail ? 1 : 2;
 #pragma unroll 1
         for (int h = 0; h < passes; ++h) {
             const uint32_t xo0 = (vg + 16 * h) * kRow, xo1 = (vg + 16 * h + 8) * kRow;
