@@ -338,72 +338,79 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
 
     // horizontal blocks: per (query, vector) the AVX2 Horizontal sum of each block. Lanes
     // (j, j + 1) of Horizontal run as one packed chain: dims j + 8 t and j + 1 + 8 t are
-    // adjacent in both staged rows.
-    for (uint32_t st = nvc; st < nst; ++st) {
-        begin_stage(st);
-        const float* qs = S.q[st & 1];
-        const float* xs = S.x[st & 1];
-        const uint32_t row = ncp + (st - nvc);
-        // two passes of 4 queries x 2 vectors (vg + 16 h, vg + 16 h + 8); a tile with at most 16
-        // vectors left (a cluster's tail) stores nothing from the second pass, which it skips
-        const int passes = tail ? 1 : 2;
+    // adjacent in both staged rows. Passes of 4 queries x NB vectors (vg + 16 h, vg + 16 h + 8):
+    // a tail tile with at most 16 vectors left runs pass 0 only, with at most 8 left one vector
+    // per thread; it stores nothing from the rest.
+    auto horizontal = [&](auto nb_tag, int passes) {
+        constexpr int NB = decltype(nb_tag)::value;
+        for (uint32_t st = nvc; st < nst; ++st) {
+            begin_stage(st);
+            const float* qs = S.q[st & 1];
+            const float* xs = S.x[st & 1];
+            const uint32_t row = ncp + (st - nvc);
 #pragma unroll 1
-        for (int h = 0; h < passes; ++h) {
-            const uint32_t xo0 = (vg + 16 * h) * kRow, xo1 = (vg + 16 * h + 8) * kRow;
-            double D0[4][2], D1[4][2], E0[4][2], E1[4][2];
-            // lane pairs in the order they combine: (0,1) + (4,5) -> s0, s1; (2,3) + (6,7) -> s2, s3
+            for (int h = 0; h < passes; ++h) {
+                const uint32_t xo0 = (vg + 16 * h) * kRow, xo1 = (vg + 16 * h + 8) * kRow;
+                double D0[4][2], D1[4][2], E0[4][2], E1[4][2];
+                // lane pairs in the order they combine: (0,1) + (4,5) -> s0, s1; (2,3) + (6,7) -> s2, s3
 #pragma unroll 1
-            for (int cp2 = 0; cp2 < 4; ++cp2) {
-                const int c = ((cp2 & 1) << 2) | ((cp2 >> 1) << 1);  // 0, 4, 2, 6
-                uint64_t a[4][2];
+                for (int cp2 = 0; cp2 < 4; ++cp2) {
+                    const int c2 = ((cp2 & 1) << 2) | ((cp2 >> 1) << 1);  // 0, 4, 2, 6
+                    uint64_t a[4][2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i][0] = a[i][1] = 0ull;
+                    for (int i = 0; i < 4; ++i) a[i][0] = a[i][1] = 0ull;
 #pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const int dim = c + 8 * t;
-                    const uint64_t x0 = *reinterpret_cast<const uint64_t*>(xs + xo0 + dim);
-                    const uint64_t x1 = *reinterpret_cast<const uint64_t*>(xs + xo1 + dim);
+                    for (int t = 0; t < 8; ++t) {
+                        const int dim = c2 + 8 * t;
+                        const uint64_t x0 = *reinterpret_cast<const uint64_t*>(xs + xo0 + dim);
+                        uint64_t x1 = 0ull;
+                        if constexpr (NB == 2) x1 = *reinterpret_cast<const uint64_t*>(xs + xo1 + dim);
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const uint64_t qv = *reinterpret_cast<const uint64_t*>(qs + (slot0 + 4 * i) * kRow + dim);
-                        uint64_t tt = f32x2_sub(qv, x0);
-                        a[i][0] = f32x2_fma(tt, tt, a[i][0]);
-                        tt = f32x2_sub(qv, x1);
-                        a[i][1] = f32x2_fma(tt, tt, a[i][1]);
+                        for (int i = 0; i < 4; ++i) {
+                            const uint64_t qv = *reinterpret_cast<const uint64_t*>(qs + (slot0 + 4 * i) * kRow + dim);
+                            uint64_t tt = f32x2_sub(qv, x0);
+                            a[i][0] = f32x2_fma(tt, tt, a[i][0]);
+                            if constexpr (NB == 2) {
+                                tt = f32x2_sub(qv, x1);
+                                a[i][1] = f32x2_fma(tt, tt, a[i][1]);
+                            }
+                        }
                     }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) {
+                            float lo, hi;
+                            f32x2_unpack(a[i][b], lo, hi);
+                            if (cp2 == 0) {          // lanes 0, 1
+                                D0[i][b] = (double)lo;
+                                D1[i][b] = (double)hi;
+                            } else if (cp2 == 1) {   // lanes 4, 5: s0, s1
+                                D0[i][b] = D0[i][b] + (double)lo;
+                                D1[i][b] = D1[i][b] + (double)hi;
+                            } else if (cp2 == 2) {   // lanes 2, 3
+                                E0[i][b] = (double)lo;
+                                E1[i][b] = (double)hi;
+                            } else {                 // lanes 6, 7: s2, s3
+                                E0[i][b] = E0[i][b] + (double)lo;
+                                E1[i][b] = E1[i][b] + (double)hi;
+                            }
+                        }
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int b = 0; b < 2; ++b) {
-                        float lo, hi;
-                        f32x2_unpack(a[i][b], lo, hi);
-                        if (cp2 == 0) {          // lanes 0, 1
-                            D0[i][b] = (double)lo;
-                            D1[i][b] = (double)hi;
-                        } else if (cp2 == 1) {   // lanes 4, 5: s0, s1
-                            D0[i][b] = D0[i][b] + (double)lo;
-                            D1[i][b] = D1[i][b] + (double)hi;
-                        } else if (cp2 == 2) {   // lanes 2, 3
-                            E0[i][b] = (double)lo;
-                            E1[i][b] = (double)hi;
-                        } else {                 // lanes 6, 7: s2, s3
-                            E0[i][b] = E0[i][b] + (double)lo;
-                            E1[i][b] = E1[i][b] + (double)hi;
-                        }
+                    for (int b = 0; b < NB; ++b) {
+                        const uint32_t v = v0 + vg + 16 * h + 8 * b;
+                        if (slot_ok(i) && v < stride)
+                            out_row(i, row)[v] = (float)((D0[i][b] + E0[i][b]) + (D1[i][b] + E1[i][b]));
                     }
             }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    const uint32_t v = v0 + vg + 16 * h + 8 * b;
-                    if (slot_ok(i) && v < stride)
-                        out_row(i, row)[v] = (float)((D0[i][b] + E0[i][b]) + (D1[i][b] + E1[i][b]));
-                }
+            __syncthreads();
         }
-        __syncthreads();
-    }
+    };
+    if (c.n - v0 <= 8u) horizontal(std::integral_constant<int, 1>(), 1);
+    else horizontal(std::integral_constant<int, 2>(), tail ? 1 : 2);
 }
 
 // -------------------------------------------------------------------------------- replay
