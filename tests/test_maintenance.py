@@ -383,3 +383,35 @@ def test_request_batches_after_maintenance(ref_cls):
             assert not set(ids[i, :cnt[i]].tolist()) & set(victims.tolist())
         ctx.close()
         ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("itype", ["pdx_tree_f32", "pdx_tree_u8"])
+def test_tombstones_in_start_and_masked_heaps(ref_cls, itype):
+    """Clusters of about 8 rows with most rows deleted and k = 10: Start pushes tombstoned slots
+    at the mask distance (searcher.hpp:169-179, 256-280) and later clusters prune against a heap
+    top that is the mask; the results, deleted ids and mask distances included, are the oracle's.
+    A cluster with every row deleted is skipped (num_embeddings == 0)."""
+    from pdx_b200 import compiled
+    rng = np.random.default_rng(13)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "ix.pdx")
+        f, gm, X = _tree_file(p, itype, d=96, n=400, nlist=50, nmeso=5, seed=12)
+        ix = compiled.load_index(p)
+        ref = ref_cls(p)
+        deleted = set()
+        for c, rid in enumerate(f.l1.row_ids):
+            drop = rid[: max(0, len(rid) - (1 if c % 3 else 0) - 1)] if c % 2 == 0 else rid[:1]
+            for v in drop:
+                ix.delete(int(v))
+                ref.delete(int(v))
+                deleted.add(int(v))
+        R = ix.prepare_queries(gm.sample(24, 3))
+        for nprobe in (1, 2, 3, 0):
+            ix.set_nprobe(nprobe)
+            ref.set_nprobe(nprobe)
+            _compare(ix, ref, R, 10, ctx=f"{itype} nprobe {nprobe}")
+            if nprobe == 1:  # the case is reached: masked slots come back, as in the reference
+                ids, _, cnt = ix.search_batch(R, 10, transformed=True)
+                assert sum(int(i) in deleted for q in range(len(R)) for i in ids[q, :cnt[q]]) > 0
+        ref.close()
