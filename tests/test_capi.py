@@ -97,3 +97,38 @@ def test_no_cpu_fallback_without_gpu():
     path, *_ = load_golden("f32_d64")
     with pytest.raises(RuntimeError, match="cuda|CUDA"):
         compiled.load_index(path)
+
+
+def test_build_and_maintenance_argument_checks():
+    """pdxg_build / pdxg_append / pdxg_delete reject bad arguments on the host, before any GPU
+    work (BuildIndex's config checks, index.hpp:27-62; the C ABI's NULL checks)."""
+    lib = compiled.library()
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((300, 64)).astype(np.float32)
+    rot = np.eye(64, dtype=np.float32)
+    out = C.c_void_p()
+    # more clusters than rows
+    rc = lib.pdxg_build(X, 300, 64, 0, 400, 0, 0, rot, 42, 10, 0, C.byref(out))
+    assert rc == compiled.PDXG_ERR_INVALID_ARGUMENT and "exceeds" in lib.pdxg_last_error().decode()
+    # meso clusters not fewer than clusters (trees)
+    rc = lib.pdxg_build(X, 300, 64, 2, 20, 20, 0, rot, 42, 10, 0, C.byref(out))
+    assert rc == compiled.PDXG_ERR_INVALID_ARGUMENT
+    # unknown index type, empty data, d out of range
+    assert lib.pdxg_build(X, 300, 64, 4, 10, 0, 0, rot, 42, 10, 0, C.byref(out)) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    assert lib.pdxg_build(X, 0, 64, 0, 10, 0, 0, rot, 42, 10, 0, C.byref(out)) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    assert lib.pdxg_build(X, 300, 0, 0, 10, 0, 0, rot, 42, 10, 0, C.byref(out)) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    # NULL index handles
+    e = np.zeros(64, np.float32)
+    assert lib.pdxg_append(None, 0, e, 0) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    assert lib.pdxg_append_batch(None, 0, 1, e, 0) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    assert lib.pdxg_delete(None, 0) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    assert lib.pdxg_maintenance_stats(None, np.zeros(6, np.uint64)) == compiled.PDXG_ERR_INVALID_ARGUMENT
+    # the Python layer: flat types refuse maintenance with the reference's message
+    ix = compiled.PDXIndex("pdx_u8", 64)
+    with pytest.raises(RuntimeError, match="Append is not implemented in PDXIndex"):
+        ix.append_batch(0, np.zeros((2, 64), np.float32))
+    tree = compiled.PDXIndex("pdx_tree_u8", 64)
+    with pytest.raises(RuntimeError, match="empty"):
+        tree.append(0, np.zeros(64, np.float32))
+    with pytest.raises(RuntimeError, match="1D"):
+        tree.append(0, np.zeros((1, 64), np.float32))
