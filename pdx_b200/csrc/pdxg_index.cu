@@ -1008,7 +1008,10 @@ int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, La
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
     if (ix->top_mode == 1) return PDXG_OK;
-    if (ix->top_mode == 0 || ix->top_mode == 3) {
+    // auto mode: a few queries (a single search, an Append) take the one-launch per-query
+    // kernel, batches the tiled form
+    const bool small = ix->top_mode == 0 && nq <= 32;
+    if ((ix->top_mode == 0 && !small) || ix->top_mode == 3) {
         int rc = run_top_level_tiled(ix, w, qp, nq, L, st, q_offset);
         if (rc || L.p.q_order) return rc;
         if (ix->top_mode == 3)
