@@ -172,3 +172,80 @@ def test_build_rejects_bad_arguments():
         compiled.build_handle(X, "pdx_tree_f32", random_rotation(64, 1), num_clusters=20, num_meso_clusters=20)
     with pytest.raises(ValueError):
         compiled.build_handle(X, "pdx_f32", random_rotation(32, 1))
+
+
+# --- the reference's tests/test_index_properties.cpp on indexes this engine builds ---
+
+def _props_data(n, d=128, seed=42):
+    gm = GaussianMixture(d, 20, 0.4, seed=seed, unit_norm=False)
+    return gm.sample(n, 0), gm.sample(50, 1)
+
+
+@pytest.mark.parametrize("itype", TYPES)
+def test_properties_cluster_ids_sizes_dims_memory(itype):
+    """ClusterRowIdsCoverAllPoints, ClusterSizeMatchesRowIdCount, GetNumDimensionsMatchesInput,
+    InMemorySizeIsPositive (test_index_properties.cpp:18-66)."""
+    X, _ = _props_data(3000)
+    ix = compiled.PDXIndex(itype, 128, normalize=True)
+    ix.build_index(X)
+    ids = np.concatenate([ix.get_cluster_row_ids(c) for c in range(ix.get_num_clusters())])
+    assert np.array_equal(np.sort(ids), np.arange(len(X)))
+    for c in range(ix.get_num_clusters()):
+        assert ix.get_cluster_size(c) == len(ix.get_cluster_row_ids(c))
+    assert ix.get_num_dimensions() == 128
+    assert ix.get_in_memory_size_in_bytes() > 0
+
+
+@pytest.mark.parametrize("itype", TYPES)
+def test_properties_knn_larger_than_data(itype):
+    """KnnLargerThanDataReturnsAvailable (test_index_properties.cpp:69-82): 5 points, k = 100."""
+    X, Q = _props_data(5)
+    ix = compiled.PDXIndex(itype, 128, normalize=True)
+    ix.build_index(X)
+    ix.set_nprobe(ix.get_num_clusters())
+    ids, _ = ix.search(Q[0], 100)
+    assert 0 < len(ids) <= 5
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8"])
+def test_properties_num_clusters_and_full_nprobe(itype):
+    """NumClustersMatchesConfig (test_index_properties.cpp:84-140): the requested cluster count,
+    and nprobe = n, n + 1 and 0 give identical results."""
+    X, Q = _props_data(3000)
+    for requested in (10, 50, 100):
+        ix = compiled.PDXIndex(itype, 128, num_clusters=requested, normalize=True)
+        ix.build_index(X)
+        assert ix.get_num_clusters() == requested
+        outs = []
+        for nprobe in (requested, requested + 1, 0):
+            ix.set_nprobe(nprobe)
+            outs.append(ix.search_batch(Q, 10))
+        for o in outs[1:]:
+            for a, b in zip(outs[0], o):
+                np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8"])
+def test_edge_single_and_two_points(itype):
+    """SinglePointIndex, TwoPointIndex (test_index_properties.cpp:151-205)."""
+    X, _ = _props_data(2, seed=3)
+    one = compiled.PDXIndex(itype, 128, num_clusters=1, normalize=True)
+    one.build_index(X[:1])
+    assert one.get_num_clusters() == 1 and one.get_cluster_size(0) == 1
+    one.set_nprobe(0)
+    ids, _ = one.search(X[0], 10)
+    assert ids.tolist() == [0]
+    two = compiled.PDXIndex(itype, 128, num_clusters=1, normalize=True)
+    two.build_index(X)
+    two.set_nprobe(0)
+    ids, ds = two.search(X[0], 2)
+    assert len(ids) == 2 and ds[0] <= ds[1] + 1e-6
+
+
+@pytest.mark.parametrize("itype", ["pdx_f32", "pdx_u8"])
+def test_edge_num_clusters_exceeds_points(itype):
+    """NumClustersExceedsNumPointsThrows (test_index_properties.cpp:207-230)."""
+    X, _ = _props_data(10)
+    ix = compiled.PDXIndex(itype, 128, num_clusters=100, normalize=True)
+    with pytest.raises(ValueError):
+        ix.build_index(X)
