@@ -4,9 +4,10 @@
 //   1. NormalizeQuery + the rotation y = x M of every row (the FP32 SIMT GEMM of the query path).
 //   2. SQ8 parameters from the global min / max of the rotated data (scalar.hpp:60-74).
 //   3. Lloyd k-means on the rotated rows: assignment = argmin over |c|^2 - 2 x.c from a BF16
-//      tensor-core GEMM (FP32 accumulation), update = FP32 sums with atomics; spherical (unit
-//      centroids) for normalized data, empty clusters re-seeded from random rows. Tree indexes
-//      cluster the L1 centroids again into meso clusters.
+//      tensor-core GEMM (FP32 accumulation), update = one block per centroid summing its rows in
+//      FP64 in row-id order (a build is reproducible); spherical (unit centroids) for normalized
+//      data, empty clusters re-seeded from seeded random rows. Tree indexes cluster the L1
+//      centroids again into meso clusters.
 //   4. QuantizeEmbedding (U8) and the compact PDX block of every cluster (StoreClusterEmbeddings,
 //      layout.hpp:12-87: vertical dims dimension-major, U8 in groups of 4 interleaved bytes,
 //      64-dim horizontal blocks row-major), written by one kernel into the file's data region.
