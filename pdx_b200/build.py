@@ -12,8 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpdx_b200.so")
 SOURCES = ["pdxg_index.cu", "pdxg_search.cu", "pdxg_toplevel.cu", "pdxg_start.cu", "pdxg_probe.cu",
-           "pdxg_rotate.cu", "pdxg_noalloc.cu", "pdxg_gemm.cu", "pdxg_build.cu"]
-HEADERS = ["pdxg_common.cuh", "pdxg_block.cuh", "pdxg_gemm.cuh"]
+           "pdxg_rotate.cu", "pdxg_noalloc.cu", "pdxg_gemm.cu", "pdxg_build.cu", "pdxg_maint.cu"]
+HEADERS = ["pdxg_common.cuh", "pdxg_block.cuh", "pdxg_gemm.cuh", "pdxg_engine.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
