@@ -1,7 +1,10 @@
 """ctypes binding of libpdx_b200.so with the reference's pybind surface.
 
 Mirrors module `pdxearch.compiled` (python/lib.cpp:6-60, include/pdx/lib/lib.hpp:15-175):
-class `PDXIndex` with the same constructor arguments and methods, and `load_index(path)`.
+class `PDXIndex` with the same constructor arguments and methods (`build_index` builds on the
+GPU, `append` / `delete` maintain tree indexes), and `load_index(path)`. Additions: batched and
+device-pointer searches, `append_batch`, `maintenance_stats`, CUDA-graph capture, the autotuner
+and serving contexts (`Context`).
 Errors map like pybind's: invalid arguments -> ValueError, everything else -> RuntimeError.
 
 There is no CPU fallback: if the CUDA engine cannot be loaded, importing this module raises.
