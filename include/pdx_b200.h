@@ -96,7 +96,10 @@ int pdxg_search(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k
 
 /* Device-resident variant of pdxg_search: every pointer is GPU memory on the index's device;
  * the work is enqueued on `stream` (a cudaStream_t, NULL = the index's own stream) and the call
- * returns without waiting. Workspace is allocated on first use and reused. */
+ * returns without waiting. Workspace is allocated on first use and reused (growing it may
+ * synchronize the device). After Append / Delete the first search enqueues the upload of the
+ * changes on its stream ahead of its kernels, without a device synchronisation; a search issued
+ * inside a stream capture while changes are pending fails with PDXG_ERR_INVALID_ARGUMENT. */
 int pdxg_search_device(pdxg_index* index, const float* queries, uint32_t nq, uint32_t k,
                        uint32_t flags, uint32_t* ids, float* distances, uint32_t* counts,
                        void* stream);
@@ -210,13 +213,21 @@ int pdxg_kernel_times_ex(pdxg_index* index, float* out, uint32_t n);
  * counterpart in the reference (whose CPU search allocates per call, searcher.hpp:601-653).
  *
  * Same arguments and results as pdxg_search_device (all pointers GPU memory; NULL stream = the
- * index's own stream), but the scratch -- work counter, query norms, rotated queries -- comes
- * from one fixed array of PDXG_NOALLOC_SCRATCH_BYTES compiled into the library; every GPU that
- * loads the library holds it until the process exits. Limit: 512 + 4*nq + 4*nq*d bytes must
- * fit (about 2,000 queries at d = 1024); larger batches fail with PDXG_ERR_CAPACITY, and with
- * PDXG_QUERY_TRANSFORMED only the work counter is used, so any nq fits. PDXG_COLLECT_STATS is
- * rejected. The first call on a device looks up the array's device address (with that device
- * current); make that first call before any stream capture. All calls share the one array and
+ * index's own stream): raw queries are rotated by the same kernels pdxg_search_device picks for
+ * the batch (the TF32x3 tensor-core GEMM for more than 8 queries at d >= 512 with rotation mode
+ * 0, else the FP32 SIMT kernels), and the search runs the same per-query decisions, so ids and
+ * distances are identical. The scratch -- work counter, GEMM wait status, query norms or the
+ * TF32 hi / lo planes, rotated queries -- comes from one fixed array of
+ * PDXG_NOALLOC_SCRATCH_BYTES compiled into the library; every GPU that loads the library holds it
+ * until the process exits. Limit for raw queries: 12*nq*d + 512 bytes with the tensor-core
+ * rotation (682 queries at d = 1024), else 4*nq*d + 4*nq + 512 (about 2,040 at d = 1024); larger
+ * batches fail with PDXG_ERR_CAPACITY. With PDXG_QUERY_TRANSFORMED only the work counter is used,
+ * so any nq fits. PDXG_COLLECT_STATS is rejected and PDXG_TIME_KERNELS ignored; an index set to
+ * the reduced-precision probe (pdxg_set_probe_mode 1 or 2) is refused with PDXG_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's device address (with that device current);
+ * make that first call before any stream capture. After Append / Delete the first search uploads
+ * the changes on its stream (no allocation, no device synchronisation); it fails with
+ * PDXG_ERR_INVALID_ARGUMENT if that stream is being captured. All calls share the one array and
  * it keeps the previous call's contents: calls whose work overlaps on the GPU (different
  * streams, or different indexes on the same GPU) race on it and must be serialised by the
  * caller. */
@@ -309,6 +320,15 @@ int pdxg_filter_release(pdxg_index* index, int32_t filter_id);
  * FP32 SIMT GEMM. pdxg_rotation_uses_tensor_cores tells which one runs. */
 int pdxg_set_rotation_mode(pdxg_index* index, uint32_t mode);
 int pdxg_rotation_uses_tensor_cores(const pdxg_index* index);
+
+/* Engine tuning, U8 indexes: how the scan (Warmup / Prune / MergeIntoHeap of PDXearch,
+ * searcher.hpp:374-566) runs after a batched Start. 0 = cluster-major when it fits (default):
+ * each cluster's first warmup step is computed once for all the queries that visit it, bounded
+ * by each query's heap top after its Start, and a warp per query replays PDXearch on those
+ * results (queries with a filter, or a Start that leaves the heap short of k, take the per-query
+ * kernel); 1 = the per-query kernel for every query. Results are identical in both modes. No
+ * counterpart in the reference. */
+int pdxg_set_scan_mode(pdxg_index* index, uint32_t mode);
 
 /* Engine tuning: threads per query CTA (64, 128, 256 or 512; 0 = automatic). */
 int pdxg_set_threads_per_query(pdxg_index* index, uint32_t threads);

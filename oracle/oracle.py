@@ -175,6 +175,10 @@ class Reference(_Base):
     def __init__(self, path: str, flavour: str = "avx2"):
         lib_path = REF_LIB if flavour == "avx2" else REF_LIB_AVX512
         if lib_path not in Reference._libs:
+            # the reference's sgemm_ comes from a pthreads OpenBLAS while its searchers run on an
+            # OpenMP pool: one BLAS thread per caller avoids the nested pools (OpenBLAS reads
+            # this when the library loads)
+            os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
             if not os.path.exists(lib_path):
                 raise FileNotFoundError(f"{lib_path} missing: run `make -C oracle ref`")
             Reference._libs[lib_path] = C.CDLL(lib_path)

@@ -58,6 +58,7 @@ def library() -> C.CDLL:
         fn("pdxg_set_nprobe", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_pruning_aggressiveness", C.c_int, vp, C.c_float)
         fn("pdxg_set_threads_per_query", C.c_int, vp, C.c_uint32)
+        fn("pdxg_set_scan_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_set_top_level_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_last_launch_count", C.c_uint32, vp)
         fn("pdxg_set_start_mode", C.c_int, vp, C.c_uint32)
@@ -428,6 +429,10 @@ class PDXIndex:
 
     def set_threads_per_query(self, threads: int) -> None:
         _check(library().pdxg_set_threads_per_query(self._handle().ptr, int(threads)))
+
+    def set_scan_mode(self, mode: int) -> None:
+        """U8 scan after a batched Start: 0 cluster-major (default), 1 the per-query kernel only."""
+        _check(library().pdxg_set_scan_mode(self._handle().ptr, int(mode)))
 
     def register_filter(self, row_ids: np.ndarray) -> int:
         """Keeps the filter of `row_ids` resident on the GPU (extension); returns its id for

@@ -151,6 +151,67 @@ __device__ __forceinline__ uint32_t next_pow2(uint32_t x) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Warp-level primitives (one warp per query in the replay kernels).
+
+// Ascending bitonic sort of N (power of two) u64 keys by one warp.
+__device__ __forceinline__ void warp_sort_u64(uint64_t* a, uint32_t N) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t size = 2; size <= N; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = lane; i < (N >> 1); i += 32) {
+                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
+                const uint32_t hi = lo + stride;
+                const bool asc = (lo & size) == 0;
+                const uint64_t x = a[lo], y = a[hi];
+                if ((x > y) == asc) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Largest heap distance and its lowest slot (LevelOps::recompute_top), on every lane. The
+// distances are non-negative floats, ordered as their bit patterns.
+__device__ __forceinline__ void warp_heap_top(const float* hd, uint32_t hsize, float& top, uint32_t& slot) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t best = 0, bs = 0xFFFFFFFFu;
+    for (uint32_t j = lane; j < hsize; j += 32) {
+        const uint32_t x = __float_as_uint(hd[j]);
+        if (bs == 0xFFFFFFFFu || x > best) {
+            best = x;
+            bs = j;
+        }
+    }
+    const uint32_t gmax = __reduce_max_sync(0xffffffffu, best);
+    slot = __reduce_min_sync(0xffffffffu, (best == gmax) ? bs : 0xFFFFFFFFu);
+    top = __uint_as_float(gmax);
+}
+
+// Exclusive prefix of x over the warp's lanes; *total receives the sum.
+__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t x, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - x;
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// ------------------------------------------------------------------------------------------
 // Distances.
 
 // avx2_computers.hpp:47-98 over one 64-dim row, 8 threads per row (sub = lane & 7): lane j

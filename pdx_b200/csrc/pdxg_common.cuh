@@ -91,6 +91,10 @@ struct SearchParams {
     const uint32_t* start_first;    // [nq] the cluster of that row
     const uint32_t* start_dist;     // [rows x start_stride]
     uint32_t start_stride;
+    // optional: only the queries q_list[0 .. *q_list_n) are searched (the rest of a batch went
+    // through the cluster-major scan, pdxg_scan.cu)
+    const uint32_t* q_list;
+    const uint32_t* q_list_n;
     // shared-memory carve-up (bytes), computed by the host
     uint32_t smem_qf, smem_qw, smem_work, smem_heap, smem_order, smem_bits, smem_total;
     uint32_t bits_cap;           // words of the survivor bitmap (work_cap / 32); the prefix follows
@@ -172,6 +176,52 @@ struct StartParams {
     uint32_t* queue;              // [1] work counter
     uint32_t* dist;               // [nq x stride] exact U8 distances
     uint32_t stride;              // >= largest L1 cluster
+};
+
+// Cluster-major scan of U8 levels (pdxg_scan.cu): the first warmup step of every (query,
+// visited cluster) pair computed per cluster for all its queries, then one warp per query
+// replaying PDXearch on those results.
+struct ScanParams {
+    const uint8_t* arena;
+    DevLevel l1;
+    const float* ratios;          // ADSampling ratio table [d]
+    const float* queries;         // prepared queries [nq x d]
+    uint32_t nq;
+    uint32_t k;                   // output row stride (the largest per-query k)
+    const uint32_t* q_k;          // optional per-query k (<= k)
+    const int32_t* filter_of;     // optional: only queries with -1 take this path
+    const uint32_t* q_order;      // [nq x q_order_stride] L1 visit orders
+    const uint32_t* q_order_count;
+    uint32_t q_order_stride;
+    const int32_t* start_row;     // batched Start (pdxg_start.cu): row of each query, -1 none
+    const uint32_t* start_first;  // [nq] the cluster of that row
+    uint32_t* start_dist;         // [rows x start_stride]; a query's row is its scratch afterwards
+    uint32_t start_stride;
+    uint32_t cp1;                 // first warmup checkpoint: min(16, d_v)
+    uint32_t g1;                  // vertical words it covers: ceil(cp1 / 4) (<= 4)
+    uint32_t nwords;              // packed query words: qw_hoff + 16 n_hblocks
+    uint32_t* qwords;             // [nq x nwords] quantized queries, packed as the scan packs them
+    uint32_t* first_i;            // [nq] position of the Start cluster in the order; ~0u: not here
+    int32_t* lim;                 // [nq] a vector is a candidate when |x|^2 - 2 q.x < lim
+    float* heap_d;                // [nq x k] the Start's pushes, in push order
+    uint32_t* heap_id;
+    uint32_t* left;               // [nq] queries left to the per-query scan kernel
+    uint32_t* left_n;             // [1] (zeroed before)
+    uint32_t* vl_count;           // [n1] visits per cluster (zeroed before)
+    uint32_t* vl;                 // [n1 x nq] visits of each cluster: q * q_order_stride + i
+    uint32_t* cl_items;           // [n1] first work item of each cluster
+    uint32_t* items;              // [2 x item bound] (cluster, query chunk)
+    uint32_t* n_items;            // [1]
+    uint32_t* queue;              // [1] work counter
+    uint32_t* bm;                 // [nq x q_order_stride x bm_words] candidate bitmaps
+    uint32_t bm_words;            // ceil(largest cluster / 32)
+    uint32_t* out_ids;            // [nq x k]
+    float* out_dists;             // [nq x k]
+    uint32_t* out_counts;         // [nq]
+    unsigned long long* stats;    // optional, SearchParams::stats layout
+    uint32_t r_heap_cap;          // replay shared memory per warp: heap entries,
+    uint32_t r_area_bytes;        // candidate offsets / final sort area,
+    uint32_t r_warp_bytes;        // and the whole per-warp region
 };
 
 }  // namespace pdxg

@@ -123,6 +123,23 @@ struct Workspace {
     float* d_qlo = nullptr;
     uint64_t qhi_cap = 0, qlo_cap = 0;
     int* d_gemm_err = nullptr;
+    // cluster-major scan (pdxg_scan.cu): packed query words, per-query state ([3 x nq + 4]:
+    // first_i | lim | left | left_n, n_items, queue), Start heaps, per-cluster visit lists and
+    // counters, work items, candidate bitmaps
+    uint32_t* d_sc_qw = nullptr;
+    uint64_t sc_qw_cap = 0;
+    uint32_t* d_sc_q = nullptr;
+    uint64_t sc_q_cap = 0;
+    uint32_t* d_sc_heap = nullptr;
+    uint64_t sc_heap_cap = 0;
+    uint32_t* d_sc_cl = nullptr;
+    uint64_t sc_cl_cap = 0;
+    uint32_t* d_sc_vl = nullptr;
+    uint64_t sc_vl_cap = 0;
+    uint32_t* d_sc_items = nullptr;
+    uint64_t sc_items_cap = 0;
+    uint32_t* d_sc_bm = nullptr;
+    uint64_t sc_bm_cap = 0;
 };
 
 // Mutable state of a tree index once Append / Delete have been used (PDXTreeIndex,
@@ -151,6 +168,8 @@ struct Maint {
     bool tomb_dirty = false;      // tombstone bitmap
     std::vector<uint32_t> dirty_rows;  // row ids whose map entries changed
     bool quiet = false;           // no search launched since the last device synchronization
+    cudaEvent_t ev_flush = nullptr;  // after the last upload of changes: later searches wait on it
+    cudaEvent_t ev_stage = nullptr;  // after the last copy out of h_stage (before it is rewritten)
     bool in_op = false;           // inside Append: its own top-level search skips the flush
     uint32_t* d_stage = nullptr;  // row-map entries (row, cluster, position) being uploaded
     uint32_t* h_stage = nullptr;  // pinned
@@ -168,6 +187,7 @@ struct Launch {
     int threads = 256;
     int grid = 1;
     uint32_t top_launches = 0;  // kernels of a separate tree top level
+    uint32_t scan_launches = 0;  // kernels of the cluster-major scan ahead of the per-query kernel
     uint32_t start_launches = 0;  // kernels of the batched Start
     uint32_t probe_launches = 0;  // kernels of the reduced-precision probe (rotation included)
 };
@@ -195,10 +215,20 @@ int ensure_ws(pdxg_index* ix, Workspace& w, uint32_t nq, uint32_t k);
 // follow PDXIndexConfig::normalize); allow_tc: the tensor-core rotation may be used.
 int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float* out, cudaStream_t st,
                 int normalize = -1, bool allow_tc = true);
+// st: the stream the search runs on (nullptr = the index's own); pending Append / Delete changes
+// are uploaded on it first (flush_maintenance).
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter, Launch& L,
-                uint32_t np_flat_max = 0xFFFFFFFFu, uint32_t top_max = 0xFFFFFFFFu, bool probe_ahead = false);
+                uint32_t np_flat_max = 0xFFFFFFFFu, uint32_t top_max = 0xFFFFFFFFu, bool probe_ahead = false,
+                cudaStream_t st = nullptr);
+// The tensor-core (TF32x3) rotation of nq queries; hi / lo are nq x d planes, err its wait status.
+bool rotation_on_tensor_cores(const pdxg_index* ix, uint32_t nq);
+int rotate_tf32x3(pdxg_index* ix, const float* q, uint32_t nq, bool norm, float* hi, float* lo, int* err,
+                  float* out, cudaStream_t st);
 int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
                   uint32_t q_offset = 0);
+// The cluster-major scan for the queries it can take (U8 level after a batched Start, visit
+// orders ahead, no tombstones); sets L.p.q_list to the rest, for the per-query kernel.
+int run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st);
 int check_index(const pdxg_index* ix);
 // Selection bitmap + passing counts of one row-id list in the device bitmap layout.
 void build_filter(const pdxg_index* ix, const uint64_t* rows, uint64_t n, uint32_t* sel, uint32_t* pass);
@@ -206,7 +236,10 @@ void build_filter(const pdxg_index* ix, const uint64_t* rows, uint64_t n, uint32
 // Append / Delete support (pdxg_maint.cu).
 int maint_prepare_save(pdxg_index* ix);
 int refresh_registered_filters(pdxg_index* ix);
-int flush_maintenance(pdxg_index* ix);
+// Enqueues the upload of what Append / Delete changed on `st` (nullptr = the index's own stream)
+// and makes `st` wait for the last such upload; fails while `st` is being captured with changes
+// pending (the upload cannot be part of a graph).
+int flush_maintenance(pdxg_index* ix, cudaStream_t st = nullptr);
 void free_maintenance(Maint& M);
 
 }  // namespace host
@@ -243,6 +276,8 @@ struct pdxg_index {
     uint32_t top_mode = 0;  // tree top level: 0 auto, 1 inside the search CTA, 2 own launch of
                             // per-query CTAs, 3 tiled (probe, partials, replay)
     uint32_t start_mode = 0;  // U8 first-cluster Start: 0 batched when it fits, 1 in the scan
+    uint32_t scan_mode = 0;   // U8 scan after a batched Start: 0 cluster-major when it fits,
+                              // 1 the per-query kernel only
     // centroid probe: 0 the reference's (exact FP32 probe / tree top-level search), 1 BF16
     // tensor-core rotation and centroid scores + widened list + FP32 rescore, 2 the same with
     // FP8-E4M3 centroid scores. Operands are built on first use.

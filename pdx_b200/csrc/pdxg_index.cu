@@ -34,6 +34,10 @@ int top_level_occupancy(size_t smem, int threads);
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
                                    cudaStream_t st);
 cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t st);
+cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st);
+uint64_t scan_item_bound(uint32_t nq, uint32_t stride, uint32_t n1);
+int scan_bitmap_occupancy();
+uint32_t scan_queries_per_cta();
 cudaError_t launch_row_sq(const float* x, uint32_t n, uint32_t d, float* out, cudaStream_t st);
 size_t probe_select_smem(uint32_t d, uint32_t n1, uint32_t cand_cap, uint32_t sort_cap);
 cudaError_t launch_probe_select(const ProbeParams& pp, cudaStream_t st);
@@ -232,7 +236,8 @@ void free_workspace(Workspace& w) {
                     w.d_top_lists, w.d_top_count, w.d_top_vals, w.d_l1_order, w.d_l1_count,
                     w.d_st_cl, w.d_st_q, w.d_st_items, w.d_st_dist, w.d_pq_b16, w.d_pq_r16, w.d_pq_r8,
                     w.d_pq_r8s, w.d_pq_scores,
-                    w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err};
+                    w.d_req, w.d_foff, w.d_rows, w.d_qhi, w.d_qlo, w.d_gemm_err, w.d_sc_qw, w.d_sc_q,
+                    w.d_sc_heap, w.d_sc_cl, w.d_sc_vl, w.d_sc_items, w.d_sc_bm};
     for (void* q : ptrs) cudaFree(q);
     w = Workspace();
 }
@@ -527,8 +532,8 @@ namespace pdxg {
 namespace host {
 
 int plan_search(pdxg_index* ix, uint32_t nq, uint32_t k, uint32_t n_order, bool any_filter,
-                Launch& L, uint32_t np_flat_max, uint32_t top_max, bool probe_ahead) {
-    if (int rc = flush_maintenance(ix)) return rc;
+                Launch& L, uint32_t np_flat_max, uint32_t top_max, bool probe_ahead, cudaStream_t st) {
+    if (int rc = flush_maintenance(ix, st)) return rc;
     SearchParams& p = L.p;
     p.arena = ix->arena;
     p.l1 = make_level(ix->l1, ix->d_cl1, ix->d_cent1, ix->base, ix->scale,
@@ -637,6 +642,29 @@ namespace {
 namespace pdxg {
 namespace host {
 
+bool rotation_on_tensor_cores(const pdxg_index* ix, uint32_t nq) {
+    // up to 8 rows (a single query, an appended row): the FP32 GEMV has the shorter latency
+    return ix->rot_tc && ix->rot_mode == 0 && nq > 8;
+}
+
+int rotate_tf32x3(pdxg_index* ix, const float* q, uint32_t nq, bool norm, float* hi, float* lo, int* err,
+                  float* out, cudaStream_t st) {
+    const uint32_t d = ix->d;
+    PDXG_CUDA(launch_split_rows(q, nq, d, norm, hi, lo, st));
+    GemmOperand a;
+    if (make_gemm_operand(a, kGemmTF32x3, hi, lo, nq, d) != 0)
+        return fail(PDXG_ERR_CUDA, "cannot encode the query tensor maps");
+    GemmArgs g{};
+    g.M = nq;
+    g.N = d;
+    g.K = d;
+    g.out = out;
+    g.ldo = d;
+    g.error = err;
+    PDXG_CUDA(launch_gemm(a, ix->rot_op, kEpiStore, g, st));
+    return PDXG_OK;
+}
+
 // normalize: -1 follows the index's is_normalized flag (queries), 0 / 1 force it (appended rows
 // follow PDXIndexConfig::normalize).
 int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float* out, cudaStream_t st,
@@ -644,8 +672,7 @@ int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float
     if (nq == 0) return PDXG_OK;
     const uint32_t d = ix->d;
     const bool norm = normalize < 0 ? ix->normalized : normalize != 0;
-    // up to 8 rows (a single query, an appended row): the FP32 GEMV has the shorter latency
-    if (allow_tc && ix->rot_tc && ix->rot_mode == 0 && nq > 8) {
+    if (allow_tc && rotation_on_tensor_cores(ix, nq)) {
         int rc;
         if ((rc = dev_grow(w.d_qhi, w.qhi_cap, (uint64_t)nq * d))) return rc;
         if ((rc = dev_grow(w.d_qlo, w.qlo_cap, (uint64_t)nq * d))) return rc;
@@ -653,19 +680,7 @@ int prepare_dev(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, float
             PDXG_CUDA(cudaMalloc(&w.d_gemm_err, sizeof(int)));
             PDXG_CUDA(cudaMemsetAsync(w.d_gemm_err, 0, sizeof(int), st));
         }
-        PDXG_CUDA(launch_split_rows(q, nq, d, norm, w.d_qhi, w.d_qlo, st));
-        GemmOperand a;
-        if (make_gemm_operand(a, kGemmTF32x3, w.d_qhi, w.d_qlo, nq, d) != 0)
-            return fail(PDXG_ERR_CUDA, "cannot encode the query tensor maps");
-        GemmArgs g{};
-        g.M = nq;
-        g.N = d;
-        g.K = d;
-        g.out = out;
-        g.ldo = d;
-        g.error = w.d_gemm_err;
-        PDXG_CUDA(launch_gemm(a, ix->rot_op, kEpiStore, g, st));
-        return PDXG_OK;
+        return rotate_tf32x3(ix, q, nq, norm, w.d_qhi, w.d_qlo, w.d_gemm_err, out, st);
     }
     PDXG_CUDA(launch_prepare_queries(q, nq, d, ix->d_rot, norm, w.d_norms, out, st));
     return PDXG_OK;
@@ -1080,6 +1095,81 @@ int run_start_batched(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq
     return PDXG_OK;
 }
 
+}  // namespace
+
+int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st) {
+    L.p.q_list = nullptr;
+    L.p.q_list_n = nullptr;
+    L.scan_launches = 0;
+    if (ix->scan_mode != 0 || !L.u8 || !L.p.start_row || !L.p.q_order || L.p.order || L.p.l1.tomb) return PDXG_OK;
+    const DevLevel& lv = L.p.l1;
+    const uint32_t n1 = lv.nclusters, stride = L.p.q_order_stride, k = L.p.k;
+    const uint32_t nwords = lv.qw_hoff + lv.n_hblocks * 16;
+    const uint32_t bm_words = (std::max(lv.max_n, 1u) + 31) / 32;
+    if ((uint64_t)nq * stride >= 0xFFFFFFFFull || (uint64_t)n1 * nq > (256ull << 20) || stride == 0) return PDXG_OK;
+    ScanParams sp{};
+    sp.r_heap_cap = (k + 3) & ~3u;
+    sp.r_area_bytes = (uint32_t)align_up(std::max<uint64_t>(2048, 8ull * next_pow2(k)), 16);
+    sp.r_warp_bytes = (uint32_t)(align_up((uint64_t)nwords * 4, 16) + 8ull * sp.r_heap_cap + sp.r_area_bytes +
+                                 align_up((uint64_t)bm_words * 4, 16));
+    if ((uint64_t)sp.r_warp_bytes * scan_queries_per_cta() + 1024 > ix->max_smem) return PDXG_OK;
+    const int occ = scan_bitmap_occupancy();
+    if (occ <= 0) return PDXG_OK;
+    const uint64_t items = scan_item_bound(nq, stride, n1);
+    int rc;
+    if ((rc = dev_grow(w.d_sc_qw, w.sc_qw_cap, (uint64_t)nq * nwords))) return rc;
+    if ((rc = dev_grow(w.d_sc_q, w.sc_q_cap, 3ull * nq + 4))) return rc;
+    if ((rc = dev_grow(w.d_sc_heap, w.sc_heap_cap, 2ull * nq * k))) return rc;
+    if ((rc = dev_grow(w.d_sc_cl, w.sc_cl_cap, 2ull * n1))) return rc;
+    if ((rc = dev_grow(w.d_sc_vl, w.sc_vl_cap, (uint64_t)n1 * nq))) return rc;
+    if ((rc = dev_grow(w.d_sc_items, w.sc_items_cap, 2 * items))) return rc;
+    if ((rc = dev_grow(w.d_sc_bm, w.sc_bm_cap, (uint64_t)nq * stride * bm_words))) return rc;
+    sp.arena = L.p.arena;
+    sp.l1 = lv;
+    sp.ratios = L.p.ratios;
+    sp.queries = L.p.queries;
+    sp.nq = nq;
+    sp.k = k;
+    sp.q_k = L.p.q_k;
+    sp.filter_of = L.p.filter_of;
+    sp.q_order = L.p.q_order;
+    sp.q_order_count = L.p.q_order_count;
+    sp.q_order_stride = stride;
+    sp.start_row = L.p.start_row;
+    sp.start_first = L.p.start_first;
+    sp.start_dist = const_cast<uint32_t*>(L.p.start_dist);
+    sp.start_stride = L.p.start_stride;
+    sp.cp1 = std::min(16u, lv.dv);
+    sp.g1 = (sp.cp1 + 3) / 4;
+    sp.nwords = nwords;
+    sp.qwords = w.d_sc_qw;
+    sp.first_i = w.d_sc_q;
+    sp.lim = reinterpret_cast<int32_t*>(w.d_sc_q + nq);
+    sp.left = w.d_sc_q + 2ull * nq;
+    sp.left_n = w.d_sc_q + 3ull * nq;
+    sp.n_items = w.d_sc_q + 3ull * nq + 1;
+    sp.queue = w.d_sc_q + 3ull * nq + 2;
+    sp.heap_d = reinterpret_cast<float*>(w.d_sc_heap);
+    sp.heap_id = w.d_sc_heap + (uint64_t)nq * k;
+    sp.vl_count = w.d_sc_cl;
+    sp.cl_items = w.d_sc_cl + n1;
+    sp.vl = w.d_sc_vl;
+    sp.items = w.d_sc_items;
+    sp.bm = w.d_sc_bm;
+    sp.bm_words = bm_words;
+    sp.out_ids = L.p.out_ids;
+    sp.out_dists = L.p.out_dists;
+    sp.out_counts = L.p.out_counts;
+    sp.stats = L.p.stats;
+    PDXG_CUDA(launch_scan(sp, occ * ix->num_sms, st));
+    L.p.q_list = sp.left;
+    L.p.q_list_n = sp.left_n;
+    L.scan_launches = 5;
+    return PDXG_OK;
+}
+
+namespace {
+
 // Core device-side search: queries/ids/dists/counts are device pointers.
 int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq, uint32_t k, uint32_t flags,
                        const uint32_t* d_order, uint32_t n_order, const uint32_t* d_sel,
@@ -1114,7 +1204,7 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     Launch L;
     const bool probe_ahead = !gemm_probe && !ix->tree && !any_filter && !d_order && nq >= kProbeAheadMinQueries &&
                              probe_exact_ok(ix);
-    rc = plan_search(ix, nq, k, n_order, any_filter, L, 0xFFFFFFFFu, 0xFFFFFFFFu, probe_ahead);
+    rc = plan_search(ix, nq, k, n_order, any_filter, L, 0xFFFFFFFFu, 0xFFFFFFFFu, probe_ahead, st);
     if (rc) return rc;
     L.p.queries = qp;
     L.p.order = d_order;
@@ -1152,9 +1242,11 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[2], st));
     if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
     launches += L.start_launches;
+    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
+    if ((rc = run_scan_cluster_major(ix, w, nq, L, st))) return rc;
+    launches += L.scan_launches;
     ix->last_launches = launches;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
-    if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     if (timed) {
         PDXG_CUDA(cudaEventRecord(ix->tev[4], st));
@@ -1165,23 +1257,39 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
 
 }  // namespace
 
-// Search on caller-provided workspace: never allocates. `norms` needs nq floats, `rotated`
-// nq * d floats (both unused with PDXG_QUERY_TRANSFORMED), `queue` one u32.
+// Whether pdxg_search_device rotates a batch of nq raw queries on the tensor cores (TF32x3), and
+// whether its probe is the reduced-precision one: the allocation-free search sizes its scratch by
+// the first and refuses the second.
+bool pdxg_rotation_on_tensor_cores(const pdxg_index* ix, uint32_t nq) { return rotation_on_tensor_cores(ix, nq); }
+bool pdxg_reduced_precision_probe(const pdxg_index* ix) { return ix->probe_mode != 0 && probe_gemm_ok(ix); }
+
+// Search on caller-provided workspace: never allocates. Raw queries are rotated as
+// pdxg_search_device rotates them: on the tensor cores (hi / lo need nq * d floats each, 16-byte
+// aligned; gemm_err one int) when pdxg_rotation_on_tensor_cores, else by the FP32 SIMT kernels
+// (norms: nq floats). `rotated` needs nq * d floats; all of these are unused with
+// PDXG_QUERY_TRANSFORMED. `queue` is one u32.
 int pdxg_search_on_workspace(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k,
-                             uint32_t flags, float* norms, float* rotated, uint32_t* queue,
-                             uint32_t* ids, float* dists, uint32_t* counts, cudaStream_t st) {
+                             uint32_t flags, float* norms, float* rotated, float* hi, float* lo,
+                             int* gemm_err, uint32_t* queue, uint32_t* ids, float* dists,
+                             uint32_t* counts, cudaStream_t st) {
     if (nq == 0) return PDXG_OK;
     if (k == 0) {
         PDXG_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, st));
         return PDXG_OK;
     }
     const float* qp = q;
+    int rc;
     if (!(flags & PDXG_QUERY_TRANSFORMED)) {
-        PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, norms, rotated, st));
+        if (rotation_on_tensor_cores(ix, nq)) {
+            PDXG_CUDA(cudaMemsetAsync(gemm_err, 0, sizeof(int), st));
+            if ((rc = rotate_tf32x3(ix, q, nq, ix->normalized, hi, lo, gemm_err, rotated, st))) return rc;
+        } else {
+            PDXG_CUDA(launch_prepare_queries(q, nq, ix->d, ix->d_rot, ix->normalized, norms, rotated, st));
+        }
         qp = rotated;
     }
     Launch L;
-    int rc = plan_search(ix, nq, k, 0, false, L);
+    rc = plan_search(ix, nq, k, 0, false, L, 0xFFFFFFFFu, 0xFFFFFFFFu, false, st);
     if (rc) return rc;
     L.p.queries = qp;
     L.p.out_ids = ids;
@@ -1280,6 +1388,8 @@ int search_host_pipelined(pdxg_index* ix, const float* queries, uint32_t nq, uin
     }
     if ((rc = run_start_batched(ix, w, L.p.queries, nq, L, st))) return rc;
     launches += L.start_launches;
+    if ((rc = run_scan_cluster_major(ix, w, nq, L, st))) return rc;
+    launches += L.scan_launches;
     ix->last_launches = launches;
     ix->last_order_stride = L.p.q_order ? k1 : 0;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
@@ -1453,6 +1563,14 @@ int pdxg_set_start_mode(pdxg_index* ix, uint32_t mode) {
     return PDXG_OK;
 }
 
+int pdxg_set_scan_mode(pdxg_index* ix, uint32_t mode) {
+    if (int rc = check_index(ix)) return rc;
+    if (mode > 1) return fail(PDXG_ERR_INVALID_ARGUMENT, "scan mode must be 0 or 1");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    ix->scan_mode = mode;
+    return PDXG_OK;
+}
+
 int pdxg_set_threads_per_query(pdxg_index* ix, uint32_t threads) {
     if (int rc = check_index(ix)) return rc;
     if (threads != 0 && threads != 64 && threads != 128 && threads != 256 && threads != 512)
@@ -1542,7 +1660,14 @@ int pdxg_graph_launch(pdxg_graph* g, void* stream) {
     if (g_alloc_gen.load() != g->gen)
         return fail(PDXG_ERR_INVALID_ARGUMENT, "the engine's buffers changed since the capture; create the graph again");
     PDXG_CUDA(cudaSetDevice(g->ix->device));
-    PDXG_CUDA(cudaGraphLaunch(g->exec, stream ? static_cast<cudaStream_t>(stream) : g->ix->stream));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->ix->stream;
+    // the upload of the last Append / Delete changes may still run on another stream
+    if (g->ix->maint && g->ix->maint->ev_flush) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        PDXG_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs == cudaStreamCaptureStatusNone) PDXG_CUDA(cudaStreamWaitEvent(st, g->ix->maint->ev_flush, 0));
+    }
+    PDXG_CUDA(cudaGraphLaunch(g->exec, st));
     return PDXG_OK;
 }
 
@@ -1958,7 +2083,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
     // the registry cannot grow (and move) between the checks below and the launch
     std::lock_guard<std::mutex> reg_lock(ix->reg_mu);
     if (int rc = refresh_registered_filters(ix)) return rc;
-    if (int rc = flush_maintenance(ix)) return rc;  // the filters' device row maps
+    if (int rc = flush_maintenance(ix, st)) return rc;  // the filters' device row maps
     // resolve every query's parameters as PDXearch / PDXTreeIndex::Search would
     const uint32_t n1 = (uint32_t)ix->l1.fc.size();
     const uint32_t n0 = (uint32_t)ix->l0.fc.size();
@@ -2055,7 +2180,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
         qp = w.d_rq;
     }
     Launch L;
-    if ((rc = plan_search(ix, nq, k_max, 0, any_filter, L, np_max, top_max))) return rc;
+    if ((rc = plan_search(ix, nq, k_max, 0, any_filter, L, np_max, top_max, false, st))) return rc;
     L.p.queries = qp;
     L.p.q_k = w.d_req;
     L.p.q_nprobe = w.d_req + nq;
@@ -2079,6 +2204,7 @@ int pdxg_search_requests(pdxg_context* ctx, const float* queries, uint32_t nq,
         if ((rc = run_top_level(ix, w, qp, nq, L, st))) return rc;
         if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
     }
+    if ((rc = run_scan_cluster_major(ix, w, nq, L, st))) return rc;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
     PDXG_CUDA(launch_search(L.p, L.u8, L.threads, L.grid, st));
     return PDXG_OK;

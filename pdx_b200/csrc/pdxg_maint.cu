@@ -226,34 +226,59 @@ int quiesce(pdxg_index* ix) {
 }  // namespace
 
 // Uploads what Append / Delete changed (cluster records, tombstone bitmap, row maps) before a
-// search launches; a no-op without pending changes.
-int pdxg::host::flush_maintenance(pdxg_index* ix) {
+// search launches; a no-op without pending changes. Stream-ordered: the copies and the row-map
+// scatter run on the search's stream after the index stream's slot writes, and every later search
+// on any stream waits for them through ev_flush. The host waits only before it rewrites the
+// pinned row-map staging, for the previous copy out of it.
+int pdxg::host::flush_maintenance(pdxg_index* ix, cudaStream_t st) {
     Maint* M = ix->maint.get();
     if (!M || M->in_op) return PDXG_OK;
+    if (!st) st = ix->stream;
     M->quiet = false;
-    if (!M->dirty) return PDXG_OK;
-    PDXG_CUDA(cudaDeviceSynchronize());  // slot writes and moves on the index's stream
-    HostLevel& lv = ix->l1;
-    if (M->records_dirty)
-        PDXG_CUDA(cudaMemcpy(ix->d_cl1, lv.meta.data(), lv.meta.size() * sizeof(DevCluster), cudaMemcpyHostToDevice));
-    if (M->tomb_dirty && lv.sel_words)
-        PDXG_CUDA(cudaMemcpy(M->d_tomb, M->tomb.data(), (size_t)lv.sel_words * 4, cudaMemcpyHostToDevice));
-    std::vector<uint32_t>& rows = M->dirty_rows;
-    for (size_t a = 0; a < rows.size(); a += kStageRows) {
-        const uint32_t m = (uint32_t)std::min<size_t>(kStageRows, rows.size() - a);
-        for (uint32_t i = 0; i < m; ++i) {
-            const uint32_t r = rows[a + i];
-            M->h_stage[3 * i] = r;
-            M->h_stage[3 * i + 1] = ix->rid_cluster[r];
-            M->h_stage[3 * i + 2] = ix->rid_pos[r];
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PDXG_CUDA(cudaStreamIsCapturing(st, &cs));
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    if (M->dirty) {
+        if (capturing)
+            return fail(PDXG_ERR_INVALID_ARGUMENT,
+                        "Append / Delete changes are pending: run one search outside stream capture first");
+        if (!M->ev_flush) PDXG_CUDA(cudaEventCreateWithFlags(&M->ev_flush, cudaEventDisableTiming));
+        if (!M->ev_stage) PDXG_CUDA(cudaEventCreateWithFlags(&M->ev_stage, cudaEventDisableTiming));
+        if (st != ix->stream) {  // slot writes and moves on the index's stream
+            PDXG_CUDA(cudaEventRecord(M->ev_flush, ix->stream));
+            PDXG_CUDA(cudaStreamWaitEvent(st, M->ev_flush, 0));
         }
-        PDXG_CUDA(cudaMemcpy(M->d_stage, M->h_stage, (size_t)m * 12, cudaMemcpyHostToDevice));
-        scatter_row_map_kernel<<<(m + 255) / 256, 256>>>(M->d_stage, m, ix->d_rid_cluster, ix->d_rid_pos);
-        PDXG_CUDA(cudaGetLastError());
-        PDXG_CUDA(cudaDeviceSynchronize());
+        HostLevel& lv = ix->l1;
+        // pageable sources: staged by the driver before the call returns
+        if (M->records_dirty)
+            PDXG_CUDA(cudaMemcpyAsync(ix->d_cl1, lv.meta.data(), lv.meta.size() * sizeof(DevCluster),
+                                      cudaMemcpyHostToDevice, st));
+        if (M->tomb_dirty && lv.sel_words)
+            PDXG_CUDA(cudaMemcpyAsync(M->d_tomb, M->tomb.data(), (size_t)lv.sel_words * 4,
+                                      cudaMemcpyHostToDevice, st));
+        std::vector<uint32_t>& rows = M->dirty_rows;
+        for (size_t a = 0; a < rows.size(); a += kStageRows) {
+            const uint32_t m = (uint32_t)std::min<size_t>(kStageRows, rows.size() - a);
+            PDXG_CUDA(cudaEventSynchronize(M->ev_stage));  // the previous copy out of h_stage
+            for (uint32_t i = 0; i < m; ++i) {
+                const uint32_t r = rows[a + i];
+                M->h_stage[3 * i] = r;
+                M->h_stage[3 * i + 1] = ix->rid_cluster[r];
+                M->h_stage[3 * i + 2] = ix->rid_pos[r];
+            }
+            PDXG_CUDA(cudaMemcpyAsync(M->d_stage, M->h_stage, (size_t)m * 12, cudaMemcpyHostToDevice, st));
+            PDXG_CUDA(cudaEventRecord(M->ev_stage, st));
+            scatter_row_map_kernel<<<(m + 255) / 256, 256, 0, st>>>(M->d_stage, m, ix->d_rid_cluster, ix->d_rid_pos);
+            PDXG_CUDA(cudaGetLastError());
+        }
+        rows.clear();
+        M->dirty = M->records_dirty = M->tomb_dirty = false;
+        PDXG_CUDA(cudaEventRecord(M->ev_flush, st));
+        return PDXG_OK;
     }
-    rows.clear();
-    M->dirty = M->records_dirty = M->tomb_dirty = false;
+    // the last upload may still run on another stream; a capture relies on the host order of
+    // pdxg_graph_launch instead (it waits on ev_flush outside the capture)
+    if (M->ev_flush && !capturing) PDXG_CUDA(cudaStreamWaitEvent(st, M->ev_flush, 0));
     return PDXG_OK;
 }
 
@@ -333,7 +358,9 @@ int enable_maintenance(pdxg_index* ix, const char* op) {
     ix->maint = std::move(M);
     if (int rc = relayout_bitmaps(ix)) return rc;
     ix->maint->quiet = true;
-    return flush_maintenance(ix);
+    if (int rc = flush_maintenance(ix)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(ix->stream));
+    return PDXG_OK;
 }
 
 // The arena holds at least `need` bytes (the whole arena moves when it grows).
@@ -632,6 +659,7 @@ int pdxg::host::maint_prepare_save(pdxg_index* ix) {
     for (uint32_t c = 0; c < ix->maint->cl.size(); ++c)
         if (int rc = compact_cluster(ix, c, ix->stream)) return rc;
     if (int rc = flush_maintenance(ix)) return rc;
+    PDXG_CUDA(cudaStreamSynchronize(ix->stream));  // Save reads the device state next
     HostLevel& lv = ix->l1;
     lv.total_vectors = 0;
     for (size_t c = 0; c < lv.meta.size(); ++c) {
@@ -649,6 +677,8 @@ int pdxg::host::maint_prepare_save(pdxg_index* ix) {
 }
 
 void pdxg::host::free_maintenance(Maint& M) {
+    if (M.ev_flush) cudaEventDestroy(M.ev_flush);
+    if (M.ev_stage) cudaEventDestroy(M.ev_stage);
     cudaFree(M.d_tomb);
     cudaFree(M.d_stage);
     cudaFree(M.d_writes);

@@ -5,8 +5,8 @@
 // device-wide synchronisation that cudaMalloc/cudaFree can cause, or a plugin may run inside a
 // process whose allocation policy it does not control. This entry point therefore runs the
 // same search kernels as pdxg_search_device, but takes its scratch space -- the queue counter,
-// the query norms and the rotated queries -- from a fixed array compiled into the library
-// instead of allocating a workspace.
+// the query norms or the TF32 hi / lo planes of the tensor-core rotation, and the rotated queries
+// -- from a fixed array compiled into the library instead of allocating a workspace.
 //
 // The array is a file-scope __device__ variable: every GPU that loads this library holds its
 // own copy (kNoAllocScratchBytes) until the process exits. In host code the symbol is only a
@@ -22,8 +22,11 @@
 
 struct pdxg_index;
 int pdxg_search_on_workspace(pdxg_index* ix, const float* q, uint32_t nq, uint32_t k,
-                             uint32_t flags, float* norms, float* rotated, uint32_t* queue,
-                             uint32_t* ids, float* dists, uint32_t* counts, cudaStream_t st);
+                             uint32_t flags, float* norms, float* rotated, float* hi, float* lo,
+                             int* gemm_err, uint32_t* queue, uint32_t* ids, float* dists,
+                             uint32_t* counts, cudaStream_t st);
+bool pdxg_rotation_on_tensor_cores(const pdxg_index* ix, uint32_t nq);
+bool pdxg_reduced_precision_probe(const pdxg_index* ix);
 int pdxg_index_device(const pdxg_index* ix);
 uint32_t pdxg_index_dims(const pdxg_index* ix);
 std::mutex& pdxg_index_mutex(pdxg_index* ix);
@@ -34,6 +37,7 @@ namespace {
 
 constexpr uint64_t kNoAllocScratchBytes = PDXG_NOALLOC_SCRATCH_BYTES;
 constexpr uint64_t kQueueBytes = 256;  // the work counter, padded to keep the rest aligned
+constexpr uint64_t kErrBytes = 256;    // the rotation GEMM's wait status, padded likewise
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -72,14 +76,24 @@ extern "C" int pdxg_search_device_noalloc(pdxg_index* index, const float* querie
     if (flags & PDXG_COLLECT_STATS)
         return pdxg_set_error(PDXG_ERR_INVALID_ARGUMENT,
                               "PDXG_COLLECT_STATS needs a workspace; use pdxg_search_device");
+    if (pdxg_reduced_precision_probe(index))
+        return pdxg_set_error(PDXG_ERR_UNSUPPORTED,
+                              "the reduced-precision probe (pdxg_set_probe_mode 1 or 2) needs a workspace; "
+                              "use pdxg_search_device");
     const uint64_t d = pdxg_index_dims(index);
     const bool rotate = !(flags & PDXG_QUERY_TRANSFORMED);
-    const uint64_t norms_bytes = rotate ? align256((uint64_t)nq * 4) : 0;
-    const uint64_t rot_bytes = rotate ? (uint64_t)nq * d * 4 : 0;
-    if (kQueueBytes + norms_bytes + rot_bytes > kNoAllocScratchBytes)
+    // raw queries are rotated exactly as pdxg_search_device rotates them: TF32x3 tensor-core
+    // planes (hi, lo) when it would use them, else the FP32 SIMT kernels (norms)
+    const bool tc = rotate && pdxg_rotation_on_tensor_cores(index, nq);
+    const uint64_t plane = align256((uint64_t)nq * d * 4);
+    const uint64_t norms_bytes = (rotate && !tc) ? align256((uint64_t)nq * 4) : 0;
+    const uint64_t rot_bytes = rotate ? plane : 0;
+    const uint64_t split_bytes = tc ? 2 * plane : 0;
+    if (kQueueBytes + kErrBytes + norms_bytes + rot_bytes + split_bytes > kNoAllocScratchBytes)
         return pdxg_set_error(PDXG_ERR_CAPACITY,
                               "batch too large for the fixed scratch of pdxg_search_device_noalloc "
-                              "(needs nq * d * 4 + nq * 4 + 512 bytes <= PDXG_NOALLOC_SCRATCH_BYTES; "
+                              "(raw queries need 12 * nq * d + 512 bytes with the tensor-core rotation, "
+                              "else 4 * nq * d + 4 * nq + 512, within PDXG_NOALLOC_SCRATCH_BYTES; "
                               "split the batch or pass PDXG_QUERY_TRANSFORMED queries)");
     std::lock_guard<std::mutex> lock(pdxg_index_mutex(index));
     const int device = pdxg_index_device(index);
@@ -88,10 +102,19 @@ extern "C" int pdxg_search_device_noalloc(pdxg_index* index, const float* querie
     unsigned char* scratch = nullptr;
     int rc = scratch_for_device(device, &scratch);
     if (rc) return rc;
-    uint32_t* queue = reinterpret_cast<uint32_t*>(scratch);
-    float* norms = reinterpret_cast<float*>(scratch + kQueueBytes);
-    float* rotated = reinterpret_cast<float*>(scratch + kQueueBytes + norms_bytes);
+    uint64_t at = 0;
+    auto carve = [&](uint64_t bytes) {
+        unsigned char* p = scratch + at;
+        at += bytes;
+        return p;
+    };
+    uint32_t* queue = reinterpret_cast<uint32_t*>(carve(kQueueBytes));
+    int* gemm_err = reinterpret_cast<int*>(carve(kErrBytes));
+    float* norms = reinterpret_cast<float*>(carve(norms_bytes));
+    float* rotated = reinterpret_cast<float*>(carve(rot_bytes));
+    float* hi = reinterpret_cast<float*>(carve(split_bytes / 2));
+    float* lo = reinterpret_cast<float*>(carve(split_bytes / 2));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : pdxg_index_stream(index);
-    return pdxg_search_on_workspace(index, queries, nq, k, flags, norms, rotated, queue, ids,
-                                    distances, counts, st);
+    return pdxg_search_on_workspace(index, queries, nq, k, flags, norms, rotated, hi, lo, gemm_err,
+                                    queue, ids, distances, counts, st);
 }

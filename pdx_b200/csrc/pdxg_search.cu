@@ -817,12 +817,14 @@ __global__ void __launch_bounds__(T) search_kernel(const __grid_constant__ Searc
     sh.order = reinterpret_cast<uint32_t*>(smem + p.smem_order);
     sh.bits = reinterpret_cast<uint32_t*>(smem + p.smem_bits);
 
+    const uint32_t n_list = p.q_list ? __ldg(p.q_list_n) : p.nq;
     for (;;) {
         if (threadIdx.x == 0) s.query = atomicAdd(p.queue, 1u);
         __syncthreads();
-        const uint32_t q = s.query;
+        const uint32_t slot = s.query;
         __syncthreads();
-        if (q >= p.nq) break;
+        if (slot >= n_list) break;
+        const uint32_t q = p.q_list ? __ldg(p.q_list + slot) : slot;
         if (threadIdx.x == 0) {
             for (int i = 0; i < 6; ++i) s.bytes[i] = 0;
             for (int i = 0; i < 3; ++i) s.cycles[i] = 0;

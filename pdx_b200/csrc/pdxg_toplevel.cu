@@ -37,25 +37,6 @@
 
 namespace pdxg {
 
-__device__ __forceinline__ void warp_sort_u64(uint64_t* a, uint32_t N) {
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t size = 2; size <= N; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t i = lane; i < (N >> 1); i += 32) {
-                const uint32_t lo = 2u * stride * (i / stride) + (i % stride);
-                const uint32_t hi = lo + stride;
-                const bool asc = (lo & size) == 0;
-                const uint64_t x = a[lo], y = a[hi];
-                if ((x > y) == asc) {
-                    a[lo] = y;
-                    a[hi] = x;
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
-
 // -------------------------------------------------------------------------------- probe
 // CTA = up to kProbeQ queries; thread (centroid c of a group of 32, lane sub of 8) runs lane
 // `sub` of Horizontal (avx2_computers.hpp:47-98: dims sub, sub + 8, ... with FMA) for every
@@ -185,12 +166,6 @@ __device__ __forceinline__ void f32x2_unpack(uint64_t v, float& lo, float& hi) {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(const __grid_constant__ TopLevelParams tp) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -414,24 +389,6 @@ __global__ void __launch_bounds__(kPartialsThreads, 2) meso_partials_kernel(cons
 }
 
 // -------------------------------------------------------------------------------- replay
-// Largest heap distance and its lowest slot (LevelOps::recompute_top), on every lane. The
-// distances are non-negative floats, ordered as their bit patterns.
-__device__ __forceinline__ void warp_heap_top(const float* hd, uint32_t hsize, float& top, uint32_t& slot) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t best = 0, bs = 0xFFFFFFFFu;
-    for (uint32_t j = lane; j < hsize; j += 32) {
-        const uint32_t x = __float_as_uint(hd[j]);
-        if (bs == 0xFFFFFFFFu || x > best) {
-            best = x;
-            bs = j;
-        }
-    }
-    const uint32_t gmax = __reduce_max_sync(0xffffffffu, best);
-    slot = __reduce_min_sync(0xffffffffu, (best == gmax) ? bs : 0xFFFFFFFFu);
-    top = __uint_as_float(gmax);
-}
-
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Shared memory of the replay: the ratio table (d floats) for the CTA, then per warp
 //   sortbuf [r_sort_cap] u64 | pre [2][r_pre_floats] | hd, hid [r_heap_cap] | dist, pos [r_work_cap]
