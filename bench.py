@@ -274,6 +274,33 @@ def ground_truth(X, Q, k, device, normalize):
     return best_i.cpu().numpy().astype(np.int64)
 
 
+def unique_bytes(ix, nq, nprobe, elem):
+    """Index bytes one batch must read at least once, from the visit orders of the last device
+    search (computed ahead of the scan): the full vectors of every cluster that is some query's
+    Start cluster (its first non-empty visited cluster), and the first warmup checkpoint's
+    vertical rows (min(16, d_v) dims) of every cluster visited after a Start. Counted once per
+    batch however many queries read them."""
+    orders, counts = ix.last_visit_orders(nq, nprobe)
+    n1 = ix.get_num_clusters()
+    size = np.array([ix.get_cluster_size(c) for c in range(n1)], np.int64)
+    d = ix.get_num_dimensions()
+    first = np.zeros(n1, bool)
+    later = np.zeros(n1, bool)
+    visits = 0
+    for i in range(nq):
+        o = orders[i, :counts[i]]
+        o = o[size[o] > 0]
+        if len(o):
+            first[o[0]] = True
+            later[o[1:]] = True
+            visits += len(o)
+    cp1 = min(16, d)
+    return {"start_rows": int(size[first].sum()) * d * elem,
+            "first_checkpoint_rows": int(size[later].sum()) * cp1 * elem,
+            "clusters_started": int(first.sum()), "clusters_visited_later": int(later.sum()),
+            "visits": visits}
+
+
 def recall_at(ids, counts, gt, k):
     hits = 0
     for i in range(len(gt)):
@@ -388,6 +415,11 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default forms")
     ap.add_argument("--no-graph", action="store_true", help="launch each step directly, not from a CUDA graph")
     ap.add_argument("--nprobe", type=int, default=None, help="override the workload's nprobe")
+    ap.add_argument("--nq", type=int, default=None, help="override the workload's batch size")
+    ap.add_argument("--scan-mode", type=int, default=None,
+                    help="U8 scan after a batched Start: 0 cluster-major (default), 1 per-query kernel")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only the warm-up and timed search steps (for ncu captures); no bench line")
     ap.add_argument("--sweep", action="store_true",
                     help="print recall@10 / QPS over an nprobe ladder and exit")
     ap.add_argument("--serve", action="store_true",
@@ -404,6 +436,8 @@ def main():
     cfg = dict(CONFIGS[args.config])
     if args.nprobe is not None:
         cfg["nprobe"] = args.nprobe
+    if args.nq is not None:
+        cfg["nq"] = args.nq
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -462,6 +496,8 @@ def main():
         ix.set_top_level_mode(args.top_mode)
     if args.rotation_mode is not None:
         ix.set_rotation_mode(args.rotation_mode)
+    if args.scan_mode is not None:
+        ix.set_scan_mode(args.scan_mode)
     probe_mode = cfg.get("probe_mode", 0) if args.probe_mode is None else args.probe_mode
     if probe_mode:
         ix.set_probe_mode(probe_mode)
@@ -493,6 +529,16 @@ def main():
             ix.search_device(q_dev.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
                              cnt_dev.data_ptr(), stream=sp)
 
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            step()
+            flush.zero_()
+        torch.cuda.synchronize()
+        log(f"profile run: {args.warmup + args.steps} steps of {nq} queries, {ix.last_launch_count()} engine "
+            f"launches per step")
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.sweep:
         gq = torch.from_numpy(Qh[:len(gt)]).to(device)
         for npb in (16, 24, 32, 40, 48, 64, 80, 96, 128, 192, 256):

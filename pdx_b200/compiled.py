@@ -374,10 +374,13 @@ class PDXIndex:
         """Durations (ms) of the last search_device(..., time_kernels=True): query preparation,
         tree top level or reduced-precision probe, batched Start, scan kernel ("scan" is the
         batched Start plus the scan kernel)."""
-        out = np.zeros(4, np.float32)
-        _check(library().pdxg_kernel_times_ex(self._handle().ptr, out.ctypes.data, 4))
+        out = np.zeros(11, np.float32)
+        _check(library().pdxg_kernel_times_ex(self._handle().ptr, out.ctypes.data, 11))
         return {"prepare": float(out[0]), "top_level": float(out[1]), "start": float(out[2]),
-                "search_kernel": float(out[3]), "scan": float(out[2] + out[3])}
+                "search_kernel": float(out[3]), "scan": float(out[2] + out[3]),
+                "scan_plan": float(out[4]), "scan_bitmap": float(out[5]), "scan_replay": float(out[6]),
+                "scan_per_query": float(out[7]), "top_probe": float(out[8]), "top_partials": float(out[9]),
+                "top_replay": float(out[10])}
 
     def set_pruning_aggressiveness(self, epsilon0: float) -> None:
         _check(library().pdxg_set_pruning_aggressiveness(self._handle().ptr, float(epsilon0)))

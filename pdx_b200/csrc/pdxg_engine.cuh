@@ -225,10 +225,11 @@ bool rotation_on_tensor_cores(const pdxg_index* ix, uint32_t nq);
 int rotate_tf32x3(pdxg_index* ix, const float* q, uint32_t nq, bool norm, float* hi, float* lo, int* err,
                   float* out, cudaStream_t st);
 int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
-                  uint32_t q_offset = 0);
+                  uint32_t q_offset = 0, bool timed = false);
 // The cluster-major scan for the queries it can take (U8 level after a batched Start, visit
 // orders ahead, no tombstones); sets L.p.q_list to the rest, for the per-query kernel.
-int run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st);
+int run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st,
+                           bool timed = false);
 int check_index(const pdxg_index* ix);
 // Selection bitmap + passing counts of one row-id list in the device bitmap layout.
 void build_filter(const pdxg_index* ix, const uint64_t* rows, uint64_t n, uint32_t* sel, uint32_t* pass);
@@ -298,8 +299,12 @@ struct pdxg_index {
     cudaStream_t stats_stream = nullptr;
     // PDXG_TIME_KERNELS marks: start, after preparation, after top level / probe, after the
     // batched Start, end
-    cudaEvent_t tev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool tev_ready = false, tev_top = false, tev_prep = false;
+    // PDXG_TIME_KERNELS: [0..4] stage boundaries (start, after query preparation, after the top
+    // level, after the batched Start, after the scan); [5..7] inside the cluster-major scan (after
+    // its planning kernels, after the bitmaps, after the replay); [8..9] inside the tiled top level
+    // (after the meso probe, after the partials)
+    cudaEvent_t tev[10] = {};
+    bool tev_ready = false, tev_top = false, tev_prep = false, tev_scan = false, tev_tiled = false;
     uint32_t last_launches = 0;  // engine kernels launched by the last search_device_impl
     uint32_t last_order_stride = 0;  // row stride of the visit orders of the last search (0: none)
     pdxg::host::Workspace ws;

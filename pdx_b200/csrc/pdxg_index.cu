@@ -32,9 +32,9 @@ cudaError_t launch_prepare_queries(const float* q, uint32_t nq, uint32_t d, cons
 cudaError_t launch_top_level(const SearchParams& p, int grid, cudaStream_t st, int threads);
 int top_level_occupancy(size_t smem, int threads);
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
-                                   cudaStream_t st);
+                                   cudaStream_t st, const cudaEvent_t* ev);
 cudaError_t launch_start_batched(const StartParams& sp, int grid, cudaStream_t st);
-cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st);
+cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st, const cudaEvent_t* ev);
 uint64_t scan_item_bound(uint32_t nq, uint32_t stride, uint32_t n1);
 int scan_bitmap_occupancy();
 uint32_t scan_queries_per_cta();
@@ -721,7 +721,7 @@ uint32_t warmup_checkpoints(uint32_t dv, uint32_t* cp, uint32_t cap) {
 // PDXG_OK with L.p.q_order unset when this index or batch does not fit its limits (the caller
 // then uses the per-query form), or an error.
 int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
-                        uint32_t q_offset = 0) {
+                        uint32_t q_offset = 0, bool timed = false) {
     const DevLevel& l0 = L.p.l0;
     const HostLevel& h0 = ix->l0;
     if (l0.d % 4 || l0.dv % 4 || l0.dv == 0 || ((uintptr_t)qp & 15) || h0.fc.empty()) return PDXG_OK;
@@ -792,7 +792,8 @@ int run_top_level_tiled(pdxg_index* ix, Workspace& w, const float* qp, uint32_t 
     tp.stats = L.p.stats;
     const uint32_t vtiles = (max_n0 + 31) / 32;
     tp.r_smem = (uint32_t)(ratio_bytes + (uint64_t)warps * wb);
-    PDXG_CUDA(launch_top_level_tiled(tp, vtiles, warps, st));
+    PDXG_CUDA(launch_top_level_tiled(tp, vtiles, warps, st, timed ? ix->tev + 8 : nullptr));
+    ix->tev_tiled = timed;
     L.top_launches = 3;
     L.p.q_order = w.d_l1_order;
     L.p.q_order_count = w.d_l1_count;
@@ -810,15 +811,16 @@ namespace pdxg {
 namespace host {
 
 int run_top_level(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq, Launch& L, cudaStream_t st,
-                  uint32_t q_offset) {
+                  uint32_t q_offset, bool timed) {
     L.p.q_order = nullptr;
     L.p.q_order_count = nullptr;
+    ix->tev_tiled = false;
     if (ix->top_mode == 1) return PDXG_OK;
     // auto mode: a few queries (a single search, an Append) take the one-launch per-query
     // kernel, batches the tiled form
     const bool small = ix->top_mode == 0 && nq <= 32;
     if ((ix->top_mode == 0 && !small) || ix->top_mode == 3) {
-        int rc = run_top_level_tiled(ix, w, qp, nq, L, st, q_offset);
+        int rc = run_top_level_tiled(ix, w, qp, nq, L, st, q_offset, timed);
         if (rc || L.p.q_order) return rc;
         if (ix->top_mode == 3)
             return fail(PDXG_ERR_CAPACITY, "tiled top level cannot run on this index or batch "
@@ -1097,10 +1099,12 @@ int run_start_batched(pdxg_index* ix, Workspace& w, const float* qp, uint32_t nq
 
 }  // namespace
 
-int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st) {
+int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq, Launch& L, cudaStream_t st,
+                                       bool timed) {
     L.p.q_list = nullptr;
     L.p.q_list_n = nullptr;
     L.scan_launches = 0;
+    ix->tev_scan = false;
     if (ix->scan_mode != 0 || !L.u8 || !L.p.start_row || !L.p.q_order || L.p.order || L.p.l1.tomb) return PDXG_OK;
     const DevLevel& lv = L.p.l1;
     const uint32_t n1 = lv.nclusters, stride = L.p.q_order_stride, k = L.p.k;
@@ -1161,7 +1165,8 @@ int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq
     sp.out_dists = L.p.out_dists;
     sp.out_counts = L.p.out_counts;
     sp.stats = L.p.stats;
-    PDXG_CUDA(launch_scan(sp, occ * ix->num_sms, st));
+    PDXG_CUDA(launch_scan(sp, occ * ix->num_sms, st, timed ? ix->tev + 5 : nullptr));
+    ix->tev_scan = timed;
     L.p.q_list = sp.left;
     L.p.q_list_n = sp.left_n;
     L.scan_launches = 5;
@@ -1228,7 +1233,7 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
         qp = L.p.queries;
         launches += L.probe_launches;
     } else if (ix->tree && !any_filter && !d_order) {
-        rc = run_top_level(ix, w, qp, nq, L, st);
+        rc = run_top_level(ix, w, qp, nq, L, st, 0, timed);
         if (rc) return rc;
         launches += L.top_launches;
     } else if (probe_ahead) {
@@ -1243,7 +1248,7 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     if ((rc = run_start_batched(ix, w, qp, nq, L, st))) return rc;
     launches += L.start_launches;
     if (timed) PDXG_CUDA(cudaEventRecord(ix->tev[3], st));
-    if ((rc = run_scan_cluster_major(ix, w, nq, L, st))) return rc;
+    if ((rc = run_scan_cluster_major(ix, w, nq, L, st, timed))) return rc;
     launches += L.scan_launches;
     ix->last_launches = launches;
     PDXG_CUDA(cudaMemsetAsync(w.d_queue, 0, sizeof(uint32_t), st));
@@ -1864,6 +1869,24 @@ int pdxg_kernel_times_ex(pdxg_index* ix, float* out, uint32_t n) {
     out[1] = ix->tev_top ? t[1] : 0.0f;
     out[2] = t[2];
     out[3] = t[3];
+    // finer: [4] scan planning (prep, lists, items), [5] bitmaps, [6] replay, [7] per-query scan
+    // kernel (all of the scan without the cluster-major form); [8] meso probe, [9] partials,
+    // [10] top-level replay (tiled top level only)
+    float f[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (ix->tev_scan) {
+        PDXG_CUDA(cudaEventElapsedTime(&f[0], ix->tev[3], ix->tev[5]));
+        PDXG_CUDA(cudaEventElapsedTime(&f[1], ix->tev[5], ix->tev[6]));
+        PDXG_CUDA(cudaEventElapsedTime(&f[2], ix->tev[6], ix->tev[7]));
+        PDXG_CUDA(cudaEventElapsedTime(&f[3], ix->tev[7], ix->tev[4]));
+    } else {
+        f[3] = t[3];
+    }
+    if (ix->tev_tiled && ix->tev_top) {
+        PDXG_CUDA(cudaEventElapsedTime(&f[4], ix->tev[1], ix->tev[8]));
+        PDXG_CUDA(cudaEventElapsedTime(&f[5], ix->tev[8], ix->tev[9]));
+        PDXG_CUDA(cudaEventElapsedTime(&f[6], ix->tev[9], ix->tev[2]));
+    }
+    for (uint32_t i = 4; i < n && i < 11; ++i) out[i] = f[i - 4];
     return PDXG_OK;
 }
 

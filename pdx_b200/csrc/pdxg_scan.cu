@@ -600,7 +600,8 @@ int scan_bitmap_occupancy() {
 
 uint32_t scan_queries_per_cta() { return kScanWarps; }
 
-cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st) {
+// ev (optional, 3 events): recorded after the planning kernels, the bitmaps and the replay.
+cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st, const cudaEvent_t* ev) {
     cudaError_t e = cudaMemsetAsync(sp.vl_count, 0, sizeof(uint32_t) * sp.l1.nclusters, st);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(sp.left_n, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
@@ -611,13 +612,17 @@ cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st) 
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     scan_plan_kernel<<<1, kScanPlanThreads, 0, st>>>(sp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
     scan_bitmap_kernel<<<bitmap_grid, kBitmapThreads, 0, st>>>(sp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return e;
     const size_t smem = (size_t)kScanWarps * sp.r_warp_bytes;
     e = cudaFuncSetAttribute(scan_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     scan_replay_kernel<<<ctas, kScanWarps * 32, smem, st>>>(sp);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 }  // namespace pdxg

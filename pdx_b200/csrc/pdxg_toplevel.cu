@@ -613,20 +613,23 @@ __global__ void top_replay_kernel(const __grid_constant__ TopLevelParams tp) {
 // -------------------------------------------------------------------------------- launch
 size_t partials_smem_bytes() { return sizeof(PartialsSmem); }
 
+// ev (optional, 2 events): recorded after the meso probe and after the partials.
 cudaError_t launch_top_level_tiled(const TopLevelParams& tp, uint32_t vtiles, int replay_warps,
-                                   cudaStream_t st) {
+                                   cudaStream_t st, const cudaEvent_t* ev) {
     cudaError_t e = cudaMemsetAsync(tp.list_count, 0, sizeof(uint32_t) * tp.l0.nclusters, st);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(meso_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tp.probe_smem);
     if (e != cudaSuccess) return e;
     meso_probe_kernel<<<(tp.nq + tp.probe_q - 1) / tp.probe_q, kProbeThreads, tp.probe_smem, st>>>(tp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
     const int psmem = (int)sizeof(PartialsSmem);
     e = cudaFuncSetAttribute(meso_partials_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem);
     if (e != cudaSuccess) return e;
     dim3 grid((tp.nq + kTQ - 1) / kTQ, tp.l0.nclusters, vtiles);
     meso_partials_kernel<<<grid, kPartialsThreads, psmem, st>>>(tp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return e;
     const size_t rsmem = tp.r_smem;
     e = cudaFuncSetAttribute(top_replay_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem);
     if (e != cudaSuccess) return e;
