@@ -595,6 +595,7 @@ def main():
     ix.search_device(prepared.data_ptr(), nq, k, ids_dev.data_ptr(), dist_dev.data_ptr(),
                      cnt_dev.data_ptr(), stream=sp, transformed=True, stats=True)
     stats = ix.last_stats()
+    scan_stats = ix.last_scan_stats()
     # the scan kernel alone: events the engine records around its own launches on `stream`
     times = []
     for i in range(args.steps):
@@ -603,6 +604,7 @@ def main():
         times.append(ix.kernel_times())
         flush.zero_()
     torch.cuda.synchronize()
+    kernels_ms = {key: round(statistics.mean(t[key] for t in times), 4) for key in times[0]}
     kern_ms = statistics.mean(t["search_kernel"] for t in times)
     start_ms = statistics.mean(t["start"] for t in times)
     top_ms = statistics.mean(t["top_level"] for t in times)
@@ -735,6 +737,8 @@ def main():
                          "batched_start_replaces_bytes": bp["start"] if batched_start else 0,
                          "top_level_bytes_l2_resident": bp["top_level"],
                          "clusters_visited": stats["clusters_visited"],
+                         "kernels_ms": kernels_ms,
+                         "scan_counters": scan_stats,
                          "bytes_by_phase": stats["bytes_by_phase"],
                          "cycles_by_phase": stats["cycles_by_phase"]},
             "cpu_baseline": cpu,

@@ -190,6 +190,14 @@ int pdxg_prepare_queries(pdxg_index* index, const float* queries, uint32_t nq, f
  * used for the roofline accounting. */
 int pdxg_get_stats(pdxg_index* index, uint64_t out[12]);
 
+/* Counters of the cluster-major scan in the last search launched with PDXG_COLLECT_STATS
+ * (synchronizes the index's stream): out[0] candidates tested (vectors below the first warmup
+ * checkpoint's bound at the heap top after the Start), out[1] of those below the bound at the
+ * heap top of their visit, out[2] visits whose warmup stopped after its first step, out[3]
+ * visits that ran the whole warmup. No counterpart in the reference; diagnostics of
+ * pdxg_set_scan_mode 0. */
+int pdxg_get_scan_stats(pdxg_index* index, uint64_t out[4]);
+
 /* Engine kernels launched by the last pdxg_search_device call on this index (query
  * preparation, tree top level and scan; memsets not counted). No counterpart in the reference. */
 uint32_t pdxg_last_launch_count(const pdxg_index* index);

@@ -88,6 +88,7 @@ def library() -> C.CDLL:
         fn("pdxg_num_embeddings", C.c_uint64, vp)
         fn("pdxg_prepare_queries", C.c_int, vp, _f32p, C.c_uint32, _f32p)
         fn("pdxg_get_stats", C.c_int, vp, _u64p)
+        fn("pdxg_get_scan_stats", C.c_int, vp, C.c_void_p)
         fn("pdxg_kernel_times", C.c_int, vp, _f32p)
         fn("pdxg_set_rotation_mode", C.c_int, vp, C.c_uint32)
         fn("pdxg_rotation_uses_tensor_cores", C.c_int, vp)
@@ -365,6 +366,13 @@ class PDXIndex:
         return {"bytes": int(out[0]), "clusters_visited": int(out[1]), "merged": int(out[2]),
                 "bytes_by_phase": {n: int(v) for n, v in zip(names, out[3:9])},
                 "cycles_by_phase": {n: int(v) for n, v in zip(["top_level", "start", "rest"], out[9:12])}}
+
+    def last_scan_stats(self) -> dict:
+        """Cluster-major scan counters of the last search_device(..., stats=True)."""
+        out = np.zeros(4, np.uint64)
+        _check(library().pdxg_get_scan_stats(self._handle().ptr, out.ctypes.data))
+        return {"candidates": int(out[0]), "first_step_survivors": int(out[1]),
+                "visits_first_step_exit": int(out[2]), "visits_full_warmup": int(out[3])}
 
     def last_launch_count(self) -> int:
         """Engine kernels launched by the last search_device call."""

@@ -20,6 +20,10 @@ constexpr int kHDim = 64;               // H_DIM_SIZE (common.hpp:45)
 constexpr int kMaxDims = 16384;         // PDX_MAX_DIMS (common.hpp:44)
 constexpr int kNumFetchSizes = 20;      // DIMENSIONS_FETCHING_SIZES (common.hpp:47-49)
 constexpr float kSelectivity = 0.80f;   // selectivity_threshold (searcher.hpp:57)
+// Counters of a search with PDXG_COLLECT_STATS: [0..11] as SearchParams::stats describes,
+// [12..15] the cluster-major scan's (candidates tested, first-step survivors, visits whose warmup
+// stops after its first step, visits that ran the whole warmup).
+constexpr int kStatsWords = 16;
 
 struct DevCluster {
     uint64_t vert_off;  // vertical block
@@ -219,6 +223,9 @@ struct ScanParams {
     float* out_dists;             // [nq x k]
     uint32_t* out_counts;         // [nq]
     unsigned long long* stats;    // optional, SearchParams::stats layout
+    uint32_t prep_qs;             // 1: the prep kernel stages each query row in shared memory
+    uint32_t prep_qs_stride;      // floats per staged row
+    uint32_t r_surv_cap;          // replay: survivors of one cluster's first warmup step it keeps
     uint32_t r_heap_cap;          // replay shared memory per warp: heap entries,
     uint32_t r_area_bytes;        // candidate offsets / final sort area,
     uint32_t r_warp_bytes;        // and the whole per-warp region

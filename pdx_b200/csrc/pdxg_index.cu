@@ -1114,8 +1114,12 @@ int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq
     ScanParams sp{};
     sp.r_heap_cap = (k + 3) & ~3u;
     sp.r_area_bytes = (uint32_t)align_up(std::max<uint64_t>(2048, 8ull * next_pow2(k)), 16);
+    // a first warmup step that ends the warmup keeps at most n - ceil(0.8 n) survivors
+    sp.r_surv_cap = (std::max(lv.max_n, 1u) / 5 + 33 + 31) / 32 * 32;
     sp.r_warp_bytes = (uint32_t)(align_up((uint64_t)nwords * 4, 16) + 8ull * sp.r_heap_cap + sp.r_area_bytes +
-                                 align_up((uint64_t)bm_words * 4, 16));
+                                 align_up((uint64_t)bm_words * 4, 16) + 8ull * sp.r_surv_cap);
+    sp.prep_qs_stride = (lv.d + 3) & ~3u;
+    sp.prep_qs = (uint64_t)scan_queries_per_cta() * sp.prep_qs_stride * 4 + 9 * 1024 <= ix->max_smem ? 1u : 0u;
     if ((uint64_t)sp.r_warp_bytes * scan_queries_per_cta() + 1024 > ix->max_smem) return PDXG_OK;
     const int occ = scan_bitmap_occupancy();
     if (occ <= 0) return PDXG_OK;
@@ -1222,8 +1226,8 @@ int search_device_impl(pdxg_index* ix, Workspace& w, const float* q, uint32_t nq
     L.p.queue = w.d_queue;
     L.p.stats = nullptr;
     if (flags & PDXG_COLLECT_STATS) {
-        if (!w.d_stats) PDXG_CUDA(cudaMalloc(&w.d_stats, 12 * sizeof(unsigned long long)));
-        PDXG_CUDA(cudaMemsetAsync(w.d_stats, 0, 12 * sizeof(unsigned long long), st));
+        if (!w.d_stats) PDXG_CUDA(cudaMalloc(&w.d_stats, kStatsWords * sizeof(unsigned long long)));
+        PDXG_CUDA(cudaMemsetAsync(w.d_stats, 0, kStatsWords * sizeof(unsigned long long), st));
         L.p.stats = w.d_stats;
         ix->stats_stream = st;
     }
@@ -1820,6 +1824,19 @@ int pdxg_prepare_queries(pdxg_index* ix, const float* queries, uint32_t nq, floa
     PDXG_CUDA(cudaMemcpyAsync(out, ix->ws.d_rq, sizeof(float) * nq * ix->d, cudaMemcpyDeviceToHost, st));
     PDXG_CUDA(cudaStreamSynchronize(st));
     return check_gemm_error(ix->ws);
+}
+
+int pdxg_get_scan_stats(pdxg_index* ix, uint64_t out[4]) {
+    if (int rc = check_index(ix)) return rc;
+    if (!out) return fail(PDXG_ERR_INVALID_ARGUMENT, "out is NULL");
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (!ix->ws.d_stats) return fail(PDXG_ERR_INVALID_ARGUMENT, "no search ran with PDXG_COLLECT_STATS");
+    PDXG_CUDA(cudaSetDevice(ix->device));
+    PDXG_CUDA(cudaStreamSynchronize(ix->stats_stream ? ix->stats_stream : ix->stream));
+    unsigned long long h[4];
+    PDXG_CUDA(cudaMemcpy(h, ix->ws.d_stats + 12, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 4; ++i) out[i] = h[i];
+    return PDXG_OK;
 }
 
 int pdxg_get_stats(pdxg_index* ix, uint64_t out[12]) {

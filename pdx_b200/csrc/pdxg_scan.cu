@@ -71,8 +71,125 @@ __device__ __forceinline__ void add_stat(const ScanParams& sp, int idx, unsigned
 }
 
 // ------------------------------------------------------------------------------------ prep
+constexpr int kRegKeys = 32;  // Start distances a prep lane keeps in registers (clusters <= 1024)
+
+// The m-th smallest of the n keys key(v) (exact radix select, 8 bits a pass; hist: 256 words of
+// this warp's shared memory).
+template <class Key>
+__device__ __forceinline__ uint32_t warp_radix_select(uint32_t n, uint32_t m, uint32_t* hist, Key key) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t prefix = 0, mask = 0, rem = m;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) hist[lane * 8 + j] = 0;
+        __syncwarp();
+        key.for_each(n, [&](uint32_t, uint32_t k) {
+            if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+        });
+        __syncwarp();
+        uint32_t loc[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            loc[j] = hist[lane * 8 + j];
+            sum += loc[j];
+        }
+        uint32_t tot;
+        const uint32_t excl = warp_exclusive_scan(sum, tot);
+        const unsigned own = __ballot_sync(0xffffffffu, excl < rem && rem <= excl + sum);
+        const uint32_t owner = __ffs(own) - 1;
+        uint32_t bin = 0, cum = excl;
+        if (lane == owner) {
+            int b = 0;
+            for (; b < 7; ++b) {
+                if (cum + loc[b] >= rem) break;
+                cum += loc[b];
+            }
+            bin = lane * 8 + b;
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        cum = __shfl_sync(0xffffffffu, cum, owner);
+        prefix |= bin << shift;
+        mask |= 0xFFu << shift;
+        rem -= cum;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+// Start distances held by the lanes: key j of a lane is vector 32 j + lane (all loads issued
+// together).
+struct RegKeys {
+    uint32_t k[kRegKeys];
+    __device__ __forceinline__ void load(const uint32_t* src, uint32_t n) {
+        const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j) {
+            const uint32_t v = 32u * j + lane;
+            k[j] = v < n ? __ldg(src + v) : 0xFFFFFFFFu;
+        }
+    }
+    template <class F>
+    __device__ __forceinline__ void for_each(uint32_t n, F f) const {
+        const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j)
+            if (32u * j + lane < n) f(32u * j + lane, k[j]);
+    }
+    // f(v0, key of v0 + lane) for the 32-vector chunks v0 = 0, 32, ... below n, in order
+    template <class F>
+    __device__ __forceinline__ void for_chunks(uint32_t n, F f) const {
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j)
+            if (32u * j < n) f(32u * j, k[j]);
+    }
+};
+
+// Start distances read from global memory (clusters larger than the register form).
+struct MemKeys {
+    const uint32_t* src;
+    template <class F>
+    __device__ __forceinline__ void for_each(uint32_t n, F f) const {
+        for (uint32_t v = threadIdx.x & 31; v < n; v += 32) f(v, src[v]);
+    }
+    template <class F>
+    __device__ __forceinline__ void for_chunks(uint32_t n, F f) const {
+        for (uint32_t v0 = 0; v0 < n; v0 += 32) {
+            const uint32_t v = v0 + (threadIdx.x & 31);
+            f(v0, v < n ? src[v] : 0xFFFFFFFFu);
+        }
+    }
+};
+
+// Start (searcher.hpp:256-280): the m smallest keys pushed in the order of
+// LevelOps::push_smallest -- the keys below the m-th in position order, then the ties at it.
+// Returns the m-th key.
+template <class Key>
+__device__ __forceinline__ uint32_t start_push(const Key& key, uint32_t n, uint32_t m, uint32_t* hist,
+                                               const uint32_t* ids, const DevLevel& lv, float* hd, uint32_t* hid) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t kth = warp_radix_select(n, m, hist, key);
+    uint32_t pushed = 0;
+    for (int pass = 0; pass < 2 && pushed < m; ++pass) {
+        key.for_chunks(n, [&](uint32_t v0, uint32_t kv) {
+            const uint32_t v = v0 + lane;
+            const bool sel = pushed < m && v < n && (pass == 0 ? kv < kth : kv == kth);
+            const unsigned b = __ballot_sync(0xffffffffu, sel);
+            const uint32_t at = pushed + __popc(b & ((1u << lane) - 1u));
+            if (sel && at < m) {
+                hd[at] = reported_u8(kv, lv);
+                hid[at] = __ldg(ids + v);
+            }
+            pushed += __popc(b);
+        });
+    }
+    return kth;
+}
+
+// Dynamic shared memory: the warps' query rows (prep_qs set: kScanWarps x d floats), staged
+// with one coalesced pass; without it the query is read from global memory.
 __global__ void __launch_bounds__(kScanWarps * 32) scan_prep_kernel(const __grid_constant__ ScanParams sp) {
     __shared__ uint32_t hist_all[kScanWarps][256];
+    extern __shared__ __align__(16) float qs_all[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t q = blockIdx.x * kScanWarps + warp;
     if (q >= sp.nq) return;  // whole warp
@@ -112,9 +229,30 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_prep_kernel(const __grid
         leave();
         return;
     }
+    const uint32_t* src = sp.start_dist + (size_t)row * sp.start_stride;
+    RegKeys rk;
+    if (n <= 32u * kRegKeys) rk.load(src, n);  // in flight while the query is quantized
     // QuantizeEmbedding (scalar.hpp:76-94) in the scan's packed word layout; |q|^2 over the
     // first checkpoint's words
     const float* qf = sp.queries + (size_t)q * lv.d;
+    if (sp.prep_qs) {
+        float* qs = qs_all + (size_t)warp * sp.prep_qs_stride;
+        for (uint32_t i0 = 0; i0 < lv.d; i0 += 128) {
+            float t[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t i = i0 + 32 * u + lane;
+                t[u] = i < lv.d ? __ldg(qf + i) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t i = i0 + 32 * u + lane;
+                if (i < lv.d) qs[i] = t[u];
+            }
+        }
+        __syncwarp();
+        qf = qs;
+    }
     uint32_t* qw = sp.qwords + (size_t)q * sp.nwords;
     uint32_t qn = 0;
     for (uint32_t w = lane; w < sp.nwords; w += 32) {
@@ -123,64 +261,11 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_prep_kernel(const __grid
         if (w < sp.g1) qn = __dp4a(word, word, qn);
     }
     qn = __reduce_add_sync(0xffffffffu, qn);
-    // Start (searcher.hpp:256-280): the m smallest distances -- exact radix select of the m-th
-    // key, then the keys below it and the ties at it, each in position order
-    const uint32_t* src = sp.start_dist + (size_t)row * sp.start_stride;
-    uint32_t prefix = 0, mask = 0, rem = m;
-    for (int shift = 24; shift >= 0; shift -= 8) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) hist[lane * 8 + j] = 0;
-        __syncwarp();
-        for (uint32_t v = lane; v < n; v += 32) {
-            const uint32_t key = src[v];
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
-        }
-        __syncwarp();
-        uint32_t loc[8], sum = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            loc[j] = hist[lane * 8 + j];
-            sum += loc[j];
-        }
-        uint32_t tot;
-        const uint32_t excl = warp_exclusive_scan(sum, tot);
-        const unsigned own = __ballot_sync(0xffffffffu, excl < rem && rem <= excl + sum);
-        const uint32_t owner = __ffs(own) - 1;
-        uint32_t bin = 0, cum = excl;
-        if (lane == owner) {
-            int b = 0;
-            for (; b < 7; ++b) {
-                if (cum + loc[b] >= rem) break;
-                cum += loc[b];
-            }
-            bin = lane * 8 + b;
-        }
-        bin = __shfl_sync(0xffffffffu, bin, owner);
-        cum = __shfl_sync(0xffffffffu, cum, owner);
-        prefix |= bin << shift;
-        mask |= 0xFFu << shift;
-        rem -= cum;
-        __syncwarp();
-    }
-    const uint32_t kth = prefix;
     const uint32_t* ids = reinterpret_cast<const uint32_t*>(sp.arena + cl.ids_off);
     float* hd = sp.heap_d + (size_t)q * sp.k;
     uint32_t* hid = sp.heap_id + (size_t)q * sp.k;
-    uint32_t pushed = 0;
-    for (int pass = 0; pass < 2 && pushed < m; ++pass) {
-        for (uint32_t v0 = 0; v0 < n && pushed < m; v0 += 32) {
-            const uint32_t v = v0 + lane;
-            const uint32_t key = v < n ? src[v] : 0xFFFFFFFFu;
-            const bool sel = v < n && (pass == 0 ? key < kth : key == kth);
-            const unsigned b = __ballot_sync(0xffffffffu, sel);
-            const uint32_t at = pushed + __popc(b & ((1u << lane) - 1u));
-            if (sel && at < m) {
-                hd[at] = reported_u8(key, lv);
-                hid[at] = __ldg(ids + v);
-            }
-            pushed += __popc(b);
-        }
-    }
+    const uint32_t kth = n <= 32u * kRegKeys ? start_push(rk, n, m, hist, ids, lv, hd, hid)
+                                             : start_push(MemKeys{src}, n, m, hist, ids, lv, hd, hid);
     if (lane == 0) {
         // heap top after the pushes: the m-th key; the first checkpoint's bound at it
         const float tau0 = reported_u8(kth, lv);
@@ -337,7 +422,8 @@ __global__ void __launch_bounds__(kBitmapThreads) scan_bitmap_kernel(const __gri
 
 // ------------------------------------------------------------------------------------ replay
 // Per-warp shared memory: qw [nwords] | hd, hid [r_heap_cap] | area [r_area_bytes] (candidate
-// offsets as u16, or the final sort) | sbits [bm_words] survivor bitmap of one cluster.
+// offsets as u16, or the final sort) | sbits [bm_words] survivor bitmap of one cluster |
+// sv_pos, sv_d [r_surv_cap] the survivors of a first warmup step and their distances.
 struct ReplayWarp {
     uint32_t* qw;
     float* hd;
@@ -345,25 +431,18 @@ struct ReplayWarp {
     uint16_t* cand;
     uint64_t* sortbuf;
     uint32_t* sbits;
+    uint32_t* sv_pos;
+    uint32_t* sv_d;
 };
 
-// Raw distance of vector v plus horizontal block b (searcher.hpp:437-540 per vector).
-__device__ __forceinline__ uint32_t scan_add_hblock(const ScanParams& sp, const DevCluster& c, const uint32_t* qw,
-                                                    uint32_t b, uint32_t v, uint32_t raw) {
-    const uint4* row = reinterpret_cast<const uint4*>(sp.arena + c.hor_off + ((size_t)b * c.n_pad + v) * kHDim);
-    const uint4* qh = reinterpret_cast<const uint4*>(qw + sp.l1.qw_hoff + b * 16);
-    uint4 x[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) x[t] = __ldg(row + t);
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const uint4 q4 = qh[t];
-        raw = sq4(q4.x, x[t].x, raw);
-        raw = sq4(q4.y, x[t].y, raw);
-        raw = sq4(q4.z, x[t].z, raw);
-        raw = sq4(q4.w, x[t].w, raw);
-    }
-    return raw;
+constexpr int kCandPerLane = 4;  // candidates a replay lane tests per memory round trip
+constexpr int kFallPerLane = 4;  // vectors a replay lane carries through a full warmup step
+
+__device__ __forceinline__ uint32_t sq16(const uint4& q, const uint4& x, uint32_t acc) {
+    acc = sq4(q.x, x.x, acc);
+    acc = sq4(q.y, x.y, acc);
+    acc = sq4(q.z, x.z, acc);
+    return sq4(q.w, x.w, acc);
 }
 
 // One survivor of the warmup bound at checkpoint cur0: the horizontal blocks, then the
@@ -374,12 +453,22 @@ __device__ __forceinline__ bool scan_follow(const ScanParams& sp, const DevClust
                                             uint32_t v, uint32_t cur0, float top, uint32_t& raw,
                                             unsigned long long& hbytes, unsigned long long& vbytes) {
     const DevLevel& lv = sp.l1;
+    const uint32_t nhb = lv.n_hblocks;
     uint32_t cur = cur0;
-    for (uint32_t b = 0; b < lv.n_hblocks; ++b) {
-        hbytes += kHDim;
-        raw = scan_add_hblock(sp, c, qw, b, v, raw);
-        cur += kHDim;
-        if (!(raw < thr_u8(top, cur, lv, sp.ratios))) return false;
+    if (nhb) {
+        const uint4* row = reinterpret_cast<const uint4*>(sp.arena + c.hor_off) + (size_t)v * 4;
+        const size_t bstride = (size_t)c.n_pad * 4;  // uint4 per block
+        for (uint32_t b = 0; b < nhb; ++b) {
+            uint4 x[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) x[t] = __ldg(row + b * bstride + t);
+            const uint4* qh = reinterpret_cast<const uint4*>(qw + lv.qw_hoff + b * 16);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) raw = sq16(qh[t], x[t], raw);
+            hbytes += kHDim;
+            cur += kHDim;
+            if (!(raw < thr_u8(top, cur, lv, sp.ratios))) return false;
+        }
     }
     const uint32_t* vert = reinterpret_cast<const uint32_t*>(sp.arena + c.vert_off);
     uint32_t cur_v = cur0;
@@ -396,8 +485,8 @@ __device__ __forceinline__ bool scan_follow(const ScanParams& sp, const DevClust
     return true;
 }
 
-// Positions of the set bits of words[w0, w0 + 32) (w < W), ascending, as offsets from 32 w0
-// into cand; returns their number.
+// Positions of the set bits of one word per lane (word index w_rel of a group of 32 words),
+// ascending, as offsets from the group's first vector into cand; returns their number.
 __device__ __forceinline__ uint32_t scan_bits_to_offsets(uint32_t word, uint32_t w_rel, uint16_t* cand) {
     uint32_t total;
     uint32_t at = warp_exclusive_scan(__popc(word), total);
@@ -410,7 +499,7 @@ __device__ __forceinline__ uint32_t scan_bits_to_offsets(uint32_t word, uint32_t
     return total;
 }
 
-__global__ void __launch_bounds__(kScanWarps * 32) scan_replay_kernel(const __grid_constant__ ScanParams sp) {
+__global__ void __launch_bounds__(kScanWarps * 32, 3) scan_replay_kernel(const __grid_constant__ ScanParams sp) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t q = blockIdx.x * kScanWarps + warp;
@@ -426,127 +515,196 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_replay_kernel(const __gr
     R.cand = reinterpret_cast<uint16_t*>(R.hid + sp.r_heap_cap);
     R.sortbuf = reinterpret_cast<uint64_t*>(R.cand);
     R.sbits = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(R.cand) + sp.r_area_bytes);
+    R.sv_pos = R.sbits + (sp.bm_words + 3) / 4 * 4;
+    R.sv_d = R.sv_pos + sp.r_surv_cap;
     const uint32_t kq = sp.q_k ? __ldg(sp.q_k + q) : sp.k;
+    const uint32_t stride = sp.q_order_stride;
     for (uint32_t w = lane; w < sp.nwords; w += 32) R.qw[w] = __ldg(sp.qwords + (size_t)q * sp.nwords + w);
     for (uint32_t j = lane; j < kq; j += 32) {
         R.hd[j] = __ldg(sp.heap_d + (size_t)q * sp.k + j);
         R.hid[j] = __ldg(sp.heap_id + (size_t)q * sp.k + j);
     }
     __syncwarp();
-    uint32_t q1[4];
-#pragma unroll
-    for (int g = 0; g < 4; ++g) q1[g] = (uint32_t)g < sp.g1 ? R.qw[g] : 0u;
+    uint4 q1 = make_uint4(0u, 0u, 0u, 0u);  // first checkpoint's query words (zero past g1)
+    q1.x = R.qw[0];
+    if (sp.g1 > 1) q1.y = R.qw[1];
+    if (sp.g1 > 2) q1.z = R.qw[2];
+    if (sp.g1 > 3) q1.w = R.qw[3];
     float top;
     uint32_t slot;
     warp_heap_top(R.hd, kq, top, slot);
     uint32_t* scratch = sp.start_dist + (size_t)__ldg(sp.start_row + q) * sp.start_stride;
-    const uint32_t* ord = sp.q_order + (size_t)q * sp.q_order_stride;
+    const uint32_t* ord = sp.q_order + (size_t)q * stride;
     const uint32_t cnt = __ldg(sp.q_order_count + q);
+    const uint32_t S = sp.r_surv_cap;
     unsigned long long b_warm = 0, b_h = 0, b_v = 0, visits = 0, merged = 0;
+    unsigned long long n_cand = 0, n_surv = 0, n_fast = 0, n_full = 0;
+
+    // Follows the lane's survivor (alive, v, raw) through Prune with the bound at `tp`, then
+    // merges the warp's survivors in lane order (MergeIntoHeap, searcher.hpp:542-566).
+    auto prune_merge = [&](const DevCluster& c, bool alive, uint32_t v, uint32_t raw, uint32_t cur, float tp) {
+        uint32_t idv = 0;
+        if (alive) {
+            alive = scan_follow(sp, c, R.qw, v, cur, tp, raw, b_h, b_v);
+            if (alive) idv = __ldg(reinterpret_cast<const uint32_t*>(sp.arena + c.ids_off) + v);
+        }
+        const float dd = reported_u8(raw, lv);
+        unsigned bal = __ballot_sync(0xffffffffu, alive);
+        merged += __popc(bal);
+        while (bal) {
+            const int l = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const float ddl = __shfl_sync(0xffffffffu, dd, l);
+            const uint32_t idl = __shfl_sync(0xffffffffu, idv, l);
+            if (ddl < top) {
+                if (lane == 0) {
+                    R.hd[slot] = ddl;
+                    R.hid[slot] = idl;
+                }
+                __syncwarp();
+                warp_heap_top(R.hd, kq, top, slot);
+            }
+        }
+    };
+
+    // the next visit's cluster record and first bitmap words, loaded one visit ahead
+    DevCluster c_nx{};
+    uint32_t bw_nx = 0;
+    auto prefetch = [&](uint32_t ii) {
+        if (ii < cnt) {
+            c_nx = lv.clusters[__ldg(ord + ii)];
+            bw_nx = lane < sp.bm_words ? __ldg(sp.bm + ((size_t)q * stride + ii) * sp.bm_words + lane) : 0u;
+        }
+    };
+    prefetch(fi + 1);
     for (uint32_t i = fi + 1; i < cnt; ++i) {
-        const uint32_t cidx = __ldg(ord + i);
-        const DevCluster c = lv.clusters[cidx];
+        const DevCluster c = c_nx;
+        const uint32_t bw0 = bw_nx;
+        prefetch(i + 1);
         const uint32_t n = c.n;
         if (n == 0) continue;  // num_embeddings == 0 (searcher.hpp:662)
         ++visits;
         const uint32_t* vert = reinterpret_cast<const uint32_t*>(sp.arena + c.vert_off);
         const uint32_t W = (n + 31) >> 5;
         const uint32_t needed = (uint32_t)ceilf(__fmul_rn(kSelectivity, (float)n));
-        const uint32_t* bmp = sp.bm + ((size_t)q * sp.q_order_stride + i) * sp.bm_words;
-        for (uint32_t w = lane; w < W; w += 32) R.sbits[w] = 0u;
-        __syncwarp();
-        // Warmup step 1 from the candidates: the exact first-checkpoint distance of each, and
-        // the survivors under the current bound
+        const uint32_t* bmp = sp.bm + ((size_t)q * stride + i) * sp.bm_words;
+        // Warmup step 1 from the candidates: the exact first-checkpoint distance of each, and the
+        // survivors under the current bound, in position order
         const uint32_t thr1 = thr_u8(top, sp.cp1, lv, sp.ratios);
         uint32_t ns = 0;
         for (uint32_t w0 = 0; w0 < W; w0 += 32) {
             const uint32_t w = w0 + lane;
-            const uint32_t total = scan_bits_to_offsets(w < W ? __ldg(bmp + w) : 0u, lane, R.cand);
-            for (uint32_t j0 = 0; j0 < total; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                bool s = false;
-                if (j < total) {
-                    const uint32_t v = w0 * 32 + R.cand[j];
-                    uint32_t d1 = 0;
+            uint32_t word = w0 == 0 ? bw0 : (w < W ? __ldg(bmp + w) : 0u);
+            if (w >= W) word = 0u;
+            const uint32_t total = scan_bits_to_offsets(word, lane, R.cand);
+            n_cand += total;
+            for (uint32_t j0 = 0; j0 < total; j0 += 32 * kCandPerLane) {
+                uint32_t v[kCandPerLane];
+                uint4 x[kCandPerLane];
 #pragma unroll
-                    for (int g = 0; g < 4; ++g)
-                        if ((uint32_t)g < sp.g1) d1 = sq4(q1[g], __ldg(vert + (size_t)g * c.n_pad + v), d1);
-                    s = d1 < thr1;
-                    if (s) {
-                        scratch[v] = d1;
-                        atomicOr(&R.sbits[v >> 5], 1u << (v & 31));
-                    }
+                for (int u = 0; u < kCandPerLane; ++u) {
+                    const uint32_t j = j0 + 32 * u + lane;
+                    v[u] = j < total ? w0 * 32 + R.cand[j] : 0xFFFFFFFFu;
+                    const bool in = v[u] != 0xFFFFFFFFu;
+                    const uint32_t* col = vert + (in ? v[u] : 0u);
+                    x[u].x = in ? __ldg(col) : 0u;
+                    x[u].y = (in && sp.g1 > 1) ? __ldg(col + (size_t)c.n_pad) : 0u;
+                    x[u].z = (in && sp.g1 > 2) ? __ldg(col + 2 * (size_t)c.n_pad) : 0u;
+                    x[u].w = (in && sp.g1 > 3) ? __ldg(col + 3 * (size_t)c.n_pad) : 0u;
                 }
-                ns += __popc(__ballot_sync(0xffffffffu, s));
+#pragma unroll
+                for (int u = 0; u < kCandPerLane; ++u) {
+                    const uint32_t d1 = sq16(q1, x[u], 0u);
+                    const bool s = v[u] != 0xFFFFFFFFu && d1 < thr1;
+                    const unsigned bal = __ballot_sync(0xffffffffu, s);
+                    const uint32_t r = ns + __popc(bal & ((1u << lane) - 1u));
+                    if (s && r < S) {
+                        R.sv_pos[r] = v[u];
+                        R.sv_d[r] = d1;
+                    }
+                    ns += __popc(bal);
+                }
             }
             __syncwarp();
         }
         b_warm += (unsigned long long)n * sp.cp1;
-        uint32_t cur = sp.cp1;
-        if (sp.cp1 < lv.dv && n - ns < needed) {
-            // the warmup continues past the first step: run it whole (searcher.hpp:374-435)
-            cur = 0;
-            uint32_t step = 0, n_pruned = 0;
-            while (n_pruned < needed && cur < lv.dv) {
-                uint32_t last = cur + c_scan_fetch[step < kNumFetchSizes ? step : kNumFetchSizes - 1];
-                if (last > lv.dv) last = lv.dv;
-                const uint32_t thr = thr_u8(top, last, lv, sp.ratios);
-                const uint32_t g0 = cur >> 2, g_end = (last + 3) >> 2;
-                uint32_t cntp = 0;
-                for (uint32_t v = lane; v < n; v += 32) {
-                    uint32_t acc = cur == 0 ? 0u : scratch[v];
-                    for (uint32_t g = g0; g < g_end; ++g) acc = sq4(R.qw[g], __ldg(vert + (size_t)g * c.n_pad + v), acc);
-                    scratch[v] = acc;
-                    cntp += acc >= thr ? 1u : 0u;
-                }
-                n_pruned = __reduce_add_sync(0xffffffffu, cntp);
-                if (cur > 0) b_warm += (unsigned long long)n * (last - cur);
-                cur = last;
-                ++step;
+        const bool exits = sp.cp1 >= lv.dv || n - ns >= needed;  // the warmup stops after step 1
+        const float tp = top;  // the bound's heap top, fixed for the whole cluster
+        n_surv += ns;
+        if (exits && ns <= S) {
+            ++n_fast;
+            // Prune and MergeIntoHeap of the survivors, 32 at a time in position order
+            for (uint32_t g0 = 0; g0 < ns; g0 += 32) {
+                const uint32_t j = g0 + lane;
+                const bool alive = j < ns;
+                prune_merge(c, alive, alive ? R.sv_pos[j] : 0u, alive ? R.sv_d[j] : 0u, sp.cp1, tp);
             }
-            const uint32_t thr = thr_u8(top, cur, lv, sp.ratios);
-            for (uint32_t v0 = 0; v0 < n; v0 += 32) {
-                const uint32_t v = v0 + lane;
-                const unsigned bal = __ballot_sync(0xffffffffu, v < n && scratch[v] < thr);
-                if (lane == 0) R.sbits[v0 >> 5] = bal;
-            }
-            __syncwarp();
+            continue;
         }
-        // Prune (searcher.hpp:437-540) and MergeIntoHeap (searcher.hpp:542-566): survivors in
-        // position order, 32 at a time, one per lane; the bound's heap top stays `tp` for the
-        // whole cluster while the merge moves the heap
-        const float tp = top;
-        const uint32_t* ids = reinterpret_cast<const uint32_t*>(sp.arena + c.ids_off);
+        // the warmup continues past its first step (or keeps more survivors than the list
+        // holds): the whole Warmup (searcher.hpp:374-435) over every vector, the running
+        // distances in the query's scratch row
+        ++n_full;
+        uint32_t cur = 0, step = 0, n_pruned = 0;
+        while (n_pruned < needed && cur < lv.dv) {
+            uint32_t last = cur + c_scan_fetch[step < kNumFetchSizes ? step : kNumFetchSizes - 1];
+            if (last > lv.dv) last = lv.dv;
+            const uint32_t thr = thr_u8(top, last, lv, sp.ratios);
+            const uint32_t g0 = cur >> 2, g_end = (last + 3) >> 2;
+            uint32_t cntp = 0;
+            for (uint32_t v0 = 0; v0 < n; v0 += 32 * kFallPerLane) {
+                uint32_t acc[kFallPerLane];
+#pragma unroll
+                for (int u = 0; u < kFallPerLane; ++u) {
+                    const uint32_t v = v0 + 32 * u + lane;
+                    acc[u] = (v < n && cur > 0) ? scratch[v] : 0u;
+                }
+                for (uint32_t g = g0; g < g_end; g += 4) {
+                    uint32_t xs[4][kFallPerLane];
+#pragma unroll
+                    for (int gg = 0; gg < 4; ++gg)
+#pragma unroll
+                        for (int u = 0; u < kFallPerLane; ++u) {
+                            const uint32_t v = v0 + 32 * u + lane;
+                            xs[gg][u] = (v < n && g + gg < g_end) ? __ldg(vert + (size_t)(g + gg) * c.n_pad + v) : 0u;
+                        }
+#pragma unroll
+                    for (int gg = 0; gg < 4; ++gg) {
+                        const uint32_t qv = g + gg < g_end ? R.qw[g + gg] : 0u;
+#pragma unroll
+                        for (int u = 0; u < kFallPerLane; ++u) acc[u] = sq4(qv, xs[gg][u], acc[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kFallPerLane; ++u) {
+                    const uint32_t v = v0 + 32 * u + lane;
+                    if (v < n) {
+                        scratch[v] = acc[u];
+                        cntp += acc[u] >= thr ? 1u : 0u;
+                    }
+                }
+            }
+            n_pruned = __reduce_add_sync(0xffffffffu, cntp);
+            if (cur > 0) b_warm += (unsigned long long)n * (last - cur);
+            cur = last;
+            ++step;
+        }
+        // Prune: the vectors below the bound at the warmup's last checkpoint, in position order
+        const uint32_t thr = thr_u8(top, cur, lv, sp.ratios);
+        for (uint32_t v0 = 0; v0 < n; v0 += 32) {
+            const uint32_t v = v0 + lane;
+            const unsigned bal = __ballot_sync(0xffffffffu, v < n && scratch[v] < thr);
+            if (lane == 0) R.sbits[v0 >> 5] = bal;
+        }
+        __syncwarp();
         for (uint32_t w0 = 0; w0 < W; w0 += 32) {
             const uint32_t w = w0 + lane;
             const uint32_t total = scan_bits_to_offsets(w < W ? R.sbits[w] : 0u, lane, R.cand);
             for (uint32_t j0 = 0; j0 < total; j0 += 32) {
                 const uint32_t j = j0 + lane;
-                bool alive = j < total;
-                uint32_t raw = 0, idv = 0;
-                if (alive) {
-                    const uint32_t v = w0 * 32 + R.cand[j];
-                    raw = scratch[v];
-                    alive = scan_follow(sp, c, R.qw, v, cur, tp, raw, b_h, b_v);
-                    if (alive) idv = __ldg(ids + v);
-                }
-                const float dd = reported_u8(raw, lv);
-                unsigned bal = __ballot_sync(0xffffffffu, alive);
-                merged += __popc(bal);
-                while (bal) {
-                    const int l = __ffs(bal) - 1;
-                    bal &= bal - 1;
-                    const float ddl = __shfl_sync(0xffffffffu, dd, l);
-                    const uint32_t idl = __shfl_sync(0xffffffffu, idv, l);
-                    if (ddl < top) {
-                        if (lane == 0) {
-                            R.hd[slot] = ddl;
-                            R.hid[slot] = idl;
-                        }
-                        __syncwarp();
-                        warp_heap_top(R.hd, kq, top, slot);
-                    }
-                }
+                const bool alive = j < total;
+                const uint32_t v = alive ? w0 * 32 + R.cand[j] : 0u;
+                prune_merge(c, alive, v, alive ? scratch[v] : 0u, cur, tp);
             }
             __syncwarp();  // cand is rewritten by the next word group
         }
@@ -573,7 +731,6 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_replay_kernel(const __gr
     }
     if (lane == 0) sp.out_counts[q] = hs;
     if (sp.stats) {
-        // block-uniform sums only on lane 0 (b_h / b_v are per lane)
         const unsigned long long h = __reduce_add_sync(0xffffffffu, (uint32_t)b_h);
         const unsigned long long vv = __reduce_add_sync(0xffffffffu, (uint32_t)b_v);
         if (lane == 0) {
@@ -583,6 +740,10 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_replay_kernel(const __gr
             add_stat(sp, 3 + kSurvivorV, vv);
             add_stat(sp, 1, visits);
             add_stat(sp, 2, merged);
+            add_stat(sp, 12, n_cand);
+            add_stat(sp, 13, n_surv);
+            add_stat(sp, 14, n_fast);
+            add_stat(sp, 15, n_full);
         }
     }
 }
@@ -606,7 +767,12 @@ cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st, 
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(sp.left_n, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     const uint32_t ctas = (sp.nq + kScanWarps - 1) / kScanWarps;
-    scan_prep_kernel<<<ctas, kScanWarps * 32, 0, st>>>(sp);
+    const size_t prep_smem = sp.prep_qs ? (size_t)kScanWarps * sp.prep_qs_stride * 4 : 0;
+    if (prep_smem) {
+        e = cudaFuncSetAttribute(scan_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prep_smem);
+        if (e != cudaSuccess) return e;
+    }
+    scan_prep_kernel<<<ctas, kScanWarps * 32, prep_smem, st>>>(sp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     scan_count_kernel<<<(sp.nq + 255) / 256, 256, 0, st>>>(sp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

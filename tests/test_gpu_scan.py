@@ -49,6 +49,30 @@ def _both_modes(ix, R, k):
     return out
 
 
+def test_stats_are_the_same_in_both_scan_forms():
+    """The algorithmic byte counts (PDXG_COLLECT_STATS) do not depend on the scan form."""
+    import torch
+    path, Q = _index("pdx_tree_u8", 256, 6000, 16, 4, 96, seed=13)
+    ix = compiled.load_index(path)
+    ix.set_nprobe(6)
+    R = torch.from_numpy(ix.prepare_queries(Q)).cuda()
+    nq, k = len(Q), 20
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    ds = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    cnt = torch.empty(nq, dtype=torch.int32, device="cuda")
+    stats = []
+    for mode in (0, 1):
+        ix.set_scan_mode(mode)
+        ix.search_device(R.data_ptr(), nq, k, ids.data_ptr(), ds.data_ptr(), cnt.data_ptr(),
+                         stream=torch.cuda.current_stream().cuda_stream, transformed=True, stats=True)
+        torch.cuda.synchronize()
+        stats.append(ix.last_stats())
+    ix.set_scan_mode(0)
+    assert stats[0]["bytes_by_phase"] == stats[1]["bytes_by_phase"]
+    assert stats[0]["clusters_visited"] == stats[1]["clusters_visited"]
+    assert stats[0]["merged"] == stats[1]["merged"]
+
+
 def _same(a, b, ctx):
     np.testing.assert_array_equal(a[2], b[2], err_msg=f"{ctx}: counts")
     for i in range(len(a[2])):

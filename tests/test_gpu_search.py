@@ -363,6 +363,7 @@ def test_batched_start_matches_scan_start(port_cls, top_mode):
         port = port_cls(p)
         ix = compiled.load_index(p)
         ix.set_top_level_mode(top_mode)
+        ix.set_scan_mode(1)  # the per-query scan in both Start forms (tests/test_gpu_scan.py covers the other)
         R = ix.prepare_queries(Q)
         Rd = torch.from_numpy(R).cuda()
         nq = len(Q)
