@@ -209,7 +209,7 @@ uint32_t pdxg_last_launch_count(const pdxg_index* index);
 int pdxg_kernel_times(pdxg_index* index, float out[3]);
 /* As pdxg_kernel_times, split finer: out[0] query preparation, out[1] tree top level or the
  * reduced-precision probe, out[2] the batched Start, out[3] the scan (n >= 4); with n >= 11 also
- * out[4] the cluster-major scan's planning kernels, out[5] its bitmaps, out[6] its replay, out[7]
+ * out[4] the cluster-major scan's prep kernel (Start pushes, visit lists), out[5] its bitmaps, out[6] its replay, out[7]
  * the per-query scan kernel, out[8] the tiled top level's meso probe, out[9] its partials, out[10]
  * its replay (0 for what did not run). */
 int pdxg_kernel_times_ex(pdxg_index* index, float* out, uint32_t n);

@@ -210,13 +210,12 @@ struct ScanParams {
     float* heap_d;                // [nq x k] the Start's pushes, in push order
     uint32_t* heap_id;
     uint32_t* left;               // [nq] queries left to the per-query scan kernel
-    uint32_t* left_n;             // [1] (zeroed before)
+    uint32_t* left_n;             // [1] (zeroed before; n_items and queue follow it)
     uint32_t* vl_count;           // [n1] visits per cluster (zeroed before)
     uint32_t* vl;                 // [n1 x nq] visits of each cluster: q * q_order_stride + i
-    uint32_t* cl_items;           // [n1] first work item of each cluster
-    uint32_t* items;              // [2 x item bound] (cluster, query chunk)
-    uint32_t* n_items;            // [1]
-    uint32_t* queue;              // [1] work counter
+    uint32_t* items;              // [2 x item bound] (cluster, chunk of 64 list entries)
+    uint32_t* n_items;            // [1] (zeroed before)
+    uint32_t* queue;              // [1] work counter (zeroed before)
     uint32_t* bm;                 // [nq x q_order_stride x bm_words] candidate bitmaps
     uint32_t bm_words;            // ceil(largest cluster / 32)
     uint32_t* out_ids;            // [nq x k]

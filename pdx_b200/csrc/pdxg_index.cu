@@ -1128,7 +1128,7 @@ int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq
     if ((rc = dev_grow(w.d_sc_qw, w.sc_qw_cap, (uint64_t)nq * nwords))) return rc;
     if ((rc = dev_grow(w.d_sc_q, w.sc_q_cap, 3ull * nq + 4))) return rc;
     if ((rc = dev_grow(w.d_sc_heap, w.sc_heap_cap, 2ull * nq * k))) return rc;
-    if ((rc = dev_grow(w.d_sc_cl, w.sc_cl_cap, 2ull * n1))) return rc;
+    if ((rc = dev_grow(w.d_sc_cl, w.sc_cl_cap, (uint64_t)n1))) return rc;
     if ((rc = dev_grow(w.d_sc_vl, w.sc_vl_cap, (uint64_t)n1 * nq))) return rc;
     if ((rc = dev_grow(w.d_sc_items, w.sc_items_cap, 2 * items))) return rc;
     if ((rc = dev_grow(w.d_sc_bm, w.sc_bm_cap, (uint64_t)nq * stride * bm_words))) return rc;
@@ -1160,7 +1160,6 @@ int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq
     sp.heap_d = reinterpret_cast<float*>(w.d_sc_heap);
     sp.heap_id = w.d_sc_heap + (uint64_t)nq * k;
     sp.vl_count = w.d_sc_cl;
-    sp.cl_items = w.d_sc_cl + n1;
     sp.vl = w.d_sc_vl;
     sp.items = w.d_sc_items;
     sp.bm = w.d_sc_bm;
@@ -1173,7 +1172,7 @@ int pdxg::host::run_scan_cluster_major(pdxg_index* ix, Workspace& w, uint32_t nq
     ix->tev_scan = timed;
     L.p.q_list = sp.left;
     L.p.q_list_n = sp.left_n;
-    L.scan_launches = 5;
+    L.scan_launches = 3;
     return PDXG_OK;
 }
 
@@ -1886,7 +1885,7 @@ int pdxg_kernel_times_ex(pdxg_index* ix, float* out, uint32_t n) {
     out[1] = ix->tev_top ? t[1] : 0.0f;
     out[2] = t[2];
     out[3] = t[3];
-    // finer: [4] scan planning (prep, lists, items), [5] bitmaps, [6] replay, [7] per-query scan
+    // finer: [4] scan prep (Start pushes, visit lists, items), [5] bitmaps, [6] replay, [7] per-query scan
     // kernel (all of the scan without the cluster-major form); [8] meso probe, [9] partials,
     // [10] top-level replay (tiled top level only)
     float f[7] = {0, 0, 0, 0, 0, 0, 0};

@@ -23,9 +23,9 @@
 //
 //   scan_prep_kernel   : warp per query -- quantized query words, the Start's pushes (the m
 //                        smallest batched-Start distances, ties by position) and tau0's bound;
-//                        queries this path does not take go to a list for the per-query kernel
-//   scan_count_kernel  : every later (query, cluster) visit appended to its cluster's list
-//   scan_plan_kernel   : one CTA -- work items of up to 64 visits of one cluster
+//                        every later visit appended to its cluster's list, with a work item per
+//                        64 list entries; queries this path does not take go to a list for the
+//                        per-query kernel
 //   scan_bitmap_kernel : persistent CTAs over the items: candidate bitmaps with dp4a, exact
 //                        |q - x|^2 = |q|^2 + |x|^2 - 2 q.x over the first checkpoint's dims
 //   scan_replay_kernel : warp per query -- Warmup / Prune / MergeIntoHeap / result
@@ -42,7 +42,6 @@ constexpr uint32_t kScanCQ = 64;         // visits per bitmap work item
 constexpr int kBitmapThreads = 256;
 constexpr int kBitmapBPW = 4;            // 32-vector blocks a bitmap warp holds at once
 constexpr int kScanWarps = 8;            // queries per prep / replay CTA
-constexpr int kScanPlanThreads = 1024;
 constexpr uint32_t kOffPath = 0xFFFFFFFFu;
 
 // DIMENSIONS_FETCHING_SIZES (common.hpp:47-49)
@@ -261,6 +260,19 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_prep_kernel(const __grid
         if (w < sp.g1) qn = __dp4a(word, word, qn);
     }
     qn = __reduce_add_sync(0xffffffffu, qn);
+    // every later non-empty visit into its cluster's list; the visit that opens a chunk of
+    // kScanCQ list entries also opens the bitmap work item of that chunk
+    for (uint32_t i = fi + 1 + lane; i < cnt; i += 32) {
+        const uint32_t c = __ldg(ord + i);
+        if (lv.clusters[c].n == 0) continue;  // num_embeddings == 0 (searcher.hpp:662)
+        const uint32_t slot = atomicAdd(sp.vl_count + c, 1u);
+        sp.vl[(size_t)c * sp.nq + slot] = q * sp.q_order_stride + i;
+        if (slot % kScanCQ == 0) {
+            const uint32_t it = atomicAdd(sp.n_items, 1u);
+            sp.items[2 * it] = c;
+            sp.items[2 * it + 1] = slot / kScanCQ;
+        }
+    }
     const uint32_t* ids = reinterpret_cast<const uint32_t*>(sp.arena + cl.ids_off);
     float* hd = sp.heap_d + (size_t)q * sp.k;
     uint32_t* hid = sp.heap_id + (size_t)q * sp.k;
@@ -277,61 +289,6 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_prep_kernel(const __grid
             add_stat(sp, 3 + kStart, (unsigned long long)n * lv.d);
             add_stat(sp, 1, 1ull);
         }
-    }
-}
-
-// ------------------------------------------------------------------------------------ lists
-__global__ void scan_count_kernel(const __grid_constant__ ScanParams sp) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= sp.nq) return;
-    const uint32_t fi = sp.first_i[q];
-    if (fi == kOffPath) return;
-    const uint32_t* ord = sp.q_order + (size_t)q * sp.q_order_stride;
-    const uint32_t cnt = sp.q_order_count[q];
-    for (uint32_t i = fi + 1; i < cnt; ++i) {
-        const uint32_t c = ord[i];
-        if (sp.l1.clusters[c].n == 0) continue;  // num_embeddings == 0 (searcher.hpp:662)
-        const uint32_t slot = atomicAdd(sp.vl_count + c, 1u);
-        sp.vl[(size_t)c * sp.nq + slot] = q * sp.q_order_stride + i;
-    }
-}
-
-__global__ void __launch_bounds__(kScanPlanThreads) scan_plan_kernel(const __grid_constant__ ScanParams sp) {
-    __shared__ uint32_t warp_tot[33];
-    const uint32_t n1 = sp.l1.nclusters;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // exclusive scan of the per-cluster item counts into cl_items
-    uint32_t carry = 0;
-    for (uint32_t b0 = 0; b0 < n1; b0 += kScanPlanThreads) {
-        const uint32_t c = b0 + threadIdx.x;
-        const uint32_t x = c < n1 ? (sp.vl_count[c] + kScanCQ - 1) / kScanCQ : 0u;
-        uint32_t tot;
-        const uint32_t excl = warp_exclusive_scan(x, tot);
-        if (lane == 0) warp_tot[warp] = tot;
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t v = warp_tot[lane];
-            uint32_t all;
-            const uint32_t e = warp_exclusive_scan(v, all);
-            warp_tot[lane] = e;
-            if (lane == 0) warp_tot[32] = all;
-        }
-        __syncthreads();
-        if (c < n1) sp.cl_items[c] = carry + warp_tot[warp] + excl;
-        carry += warp_tot[32];
-        __syncthreads();
-    }
-    for (uint32_t c = threadIdx.x; c < n1; c += kScanPlanThreads) {
-        const uint32_t chunks = (sp.vl_count[c] + kScanCQ - 1) / kScanCQ;
-        uint32_t it = sp.cl_items[c];
-        for (uint32_t a = 0; a < chunks; ++a, ++it) {
-            sp.items[2 * it] = c;
-            sp.items[2 * it + 1] = a;
-        }
-    }
-    if (threadIdx.x == 0) {
-        sp.n_items[0] = carry;
-        sp.queue[0] = 0;
     }
 }
 
@@ -761,11 +718,12 @@ int scan_bitmap_occupancy() {
 
 uint32_t scan_queries_per_cta() { return kScanWarps; }
 
-// ev (optional, 3 events): recorded after the planning kernels, the bitmaps and the replay.
+// ev (optional, 3 events): recorded after the prep kernel, the bitmaps and the replay.
 cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st, const cudaEvent_t* ev) {
     cudaError_t e = cudaMemsetAsync(sp.vl_count, 0, sizeof(uint32_t) * sp.l1.nclusters, st);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(sp.left_n, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    // left_n, n_items and queue are consecutive
+    if ((e = cudaMemsetAsync(sp.left_n, 0, 3 * sizeof(uint32_t), st)) != cudaSuccess) return e;
     const uint32_t ctas = (sp.nq + kScanWarps - 1) / kScanWarps;
     const size_t prep_smem = sp.prep_qs ? (size_t)kScanWarps * sp.prep_qs_stride * 4 : 0;
     if (prep_smem) {
@@ -773,10 +731,6 @@ cudaError_t launch_scan(const ScanParams& sp, int bitmap_grid, cudaStream_t st, 
         if (e != cudaSuccess) return e;
     }
     scan_prep_kernel<<<ctas, kScanWarps * 32, prep_smem, st>>>(sp);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    scan_count_kernel<<<(sp.nq + 255) / 256, 256, 0, st>>>(sp);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    scan_plan_kernel<<<1, kScanPlanThreads, 0, st>>>(sp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
     scan_bitmap_kernel<<<bitmap_grid, kBitmapThreads, 0, st>>>(sp);
